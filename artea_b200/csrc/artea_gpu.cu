@@ -1,0 +1,597 @@
+// C-ABI of the B200 query path: device-resident index, routers, launches.
+// The kernels live in search.cuh; this file owns memory, streams, launch
+// configuration, the autotuner and the host-buffer entry points.
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/artea_gpu.h"
+#include "common.h"
+#include "search.cuh"
+
+namespace artea_gpu {
+
+namespace {
+thread_local std::string t_last_error;
+}
+
+int fail(int code, const std::string& msg) {
+    t_last_error = msg;
+    return code;
+}
+
+}  // namespace artea_gpu
+
+using artea_gpu::fail;
+
+#define CUDA_TRY(expr)                                                                              \
+    do {                                                                                            \
+        cudaError_t _e = (expr);                                                                    \
+        if (_e != cudaSuccess) return fail(ARTEA_GPU_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+struct artea_gpu_index {
+    int device = 0;
+    uint32_t n = 0, dim = 0, top = artea_gpu::kInvalidLevel, entry = 0, ul = 0, bl = 0;
+    float* d_vecs = nullptr;
+    uint2* d_vinfo = nullptr;
+    uint32_t* d_nbrs = nullptr;
+    uint64_t* d_offsets = nullptr;
+    const uint64_t* group_ptr[artea_gpu::kMaxGroups] = {};
+    uint64_t bytes = 0;
+};
+
+struct LaunchShape {
+    uint32_t warps_per_cta = 0;
+    uint32_t ctas = 0;        // grid size (persistent)
+    uint32_t slots = 0;       // visited slots needed
+};
+
+struct artea_gpu_router {
+    artea_gpu_index* idx = nullptr;
+    uint32_t topk = 0, queue = 0, max_queue = 0, cap = 0, max_batch = 0;
+    int metric = 0, mode = 0, schedule = 0;
+    uint32_t want_warps = 0, want_ctas_per_sm = 0;
+    bool use_graphs = false;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+
+    // Visited slots.
+    uint32_t* d_vis_bits = nullptr;
+    uint32_t* d_vis_list = nullptr;
+    uint32_t slots = 0;
+    uint64_t words_per_slot = 0;
+    uint32_t list_cap = 0;
+
+    uint32_t* d_counter = nullptr;
+    int* d_error = nullptr;
+
+    // Staging for host-buffer calls.
+    float* d_queries = nullptr;
+    uint64_t* d_out = nullptr;
+    uint32_t* d_topk = nullptr;
+    uint32_t* d_queue = nullptr;
+    artea_gpu_query_stats* d_stats = nullptr;
+    uint32_t stage_nq = 0, stage_kstride = 0;
+
+    uint64_t launches = 0;
+    std::map<uint64_t, uint32_t> tuned_warps;   // (dim, max queue) -> warps per CTA
+    std::map<uint32_t, LaunchShape> shapes;     // warps per CTA -> persistent grid
+};
+
+namespace {
+
+using namespace artea_gpu;
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+template <typename T>
+int dev_alloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) return ARTEA_GPU_OK;
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * count);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? ARTEA_GPU_ENOMEM : ARTEA_GPU_ECUDA,
+                    std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return ARTEA_GPU_OK;
+}
+
+template <typename T>
+void dev_free(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+using KernelFn = void (*)(SearchArgs);
+
+template <int kMetric>
+KernelFn pick_kernel_m(bool exact, bool persistent) {
+    if (persistent) return exact ? search_persistent_kernel<kMetric, true> : search_persistent_kernel<kMetric, false>;
+    return exact ? search_plain_kernel<kMetric, true> : search_plain_kernel<kMetric, false>;
+}
+
+KernelFn pick_kernel(int metric, bool exact, bool persistent) {
+    switch (metric) {
+        case ARTEA_GPU_EUCLIDEAN_SQR: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN_SQR>(exact, persistent);
+        case ARTEA_GPU_EUCLIDEAN: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN>(exact, persistent);
+        case ARTEA_GPU_COSINE: return pick_kernel_m<ARTEA_GPU_COSINE>(exact, persistent);
+        case ARTEA_GPU_DOT: return pick_kernel_m<ARTEA_GPU_DOT>(exact, persistent);
+        default: return nullptr;
+    }
+}
+
+uint32_t smem_bytes_per_warp(uint32_t dim, uint32_t cap) { return warp_smem_words(dim, cap) * 4u; }
+
+int ensure_slots(artea_gpu_router* r, uint32_t slots) {
+    if (slots <= r->slots) return ARTEA_GPU_OK;
+    dev_free(r->d_vis_bits);
+    dev_free(r->d_vis_list);
+    r->slots = 0;
+    const size_t words = r->words_per_slot * slots;
+    if (int rc = dev_alloc(&r->d_vis_bits, words)) return rc;
+    if (int rc = dev_alloc(&r->d_vis_list, static_cast<size_t>(r->list_cap) * slots)) return rc;
+    CUDA_TRY(cudaMemsetAsync(r->d_vis_bits, 0, sizeof(uint32_t) * words, r->stream));
+    r->slots = slots;
+    return ARTEA_GPU_OK;
+}
+
+int ensure_stage(artea_gpu_router* r, uint32_t nq, uint32_t k_stride) {
+    if (nq <= r->stage_nq && k_stride <= r->stage_kstride) return ARTEA_GPU_OK;
+    const uint32_t n2 = std::max(nq, r->stage_nq);
+    const uint32_t k2 = std::max(k_stride, r->stage_kstride);
+    dev_free(r->d_queries);
+    dev_free(r->d_out);
+    dev_free(r->d_topk);
+    dev_free(r->d_queue);
+    dev_free(r->d_stats);
+    r->stage_nq = r->stage_kstride = 0;
+    if (int rc = dev_alloc(&r->d_queries, static_cast<size_t>(n2) * r->idx->dim)) return rc;
+    if (int rc = dev_alloc(&r->d_out, static_cast<size_t>(n2) * k2)) return rc;
+    if (int rc = dev_alloc(&r->d_topk, n2)) return rc;
+    if (int rc = dev_alloc(&r->d_queue, n2)) return rc;
+    if (int rc = dev_alloc(&r->d_stats, n2)) return rc;
+    r->stage_nq = n2;
+    r->stage_kstride = k2;
+    return ARTEA_GPU_OK;
+}
+
+// Persistent grid for a warp count: as many CTAs per SM as fit.
+int persistent_shape(artea_gpu_router* r, uint32_t warps, LaunchShape* s) {
+    auto hit = r->shapes.find(warps);
+    if (hit != r->shapes.end()) {
+        *s = hit->second;
+        return ARTEA_GPU_OK;
+    }
+    KernelFn fn = pick_kernel(r->metric, r->mode == ARTEA_GPU_MODE_EXACT, true);
+    const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap) * warps;
+    CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(fn),
+                                                           static_cast<int>(warps * 32), smem));
+    if (per_sm <= 0) return fail(ARTEA_GPU_EINVAL, "persistent kernel does not fit on an SM (queue too large?)");
+    if (r->want_ctas_per_sm) per_sm = std::min<int>(per_sm, static_cast<int>(r->want_ctas_per_sm));
+    s->warps_per_cta = warps;
+    s->ctas = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(r->num_sms);
+    s->slots = s->ctas * warps;
+    r->shapes[warps] = *s;
+    return ARTEA_GPU_OK;
+}
+
+int fill_args(artea_gpu_router* r, SearchArgs* a, const float* d_q, uint32_t nq, const uint32_t* d_topk,
+              const uint32_t* d_queue, uint32_t k_stride, uint64_t* d_out, artea_gpu_query_stats* d_stats,
+              bool l0_only) {
+    const artea_gpu_index* ix = r->idx;
+    std::memset(a, 0, sizeof(*a));
+    a->g.vecs = ix->d_vecs;
+    a->g.vinfo = ix->d_vinfo;
+    a->g.nbrs = ix->d_nbrs;
+    a->g.n = ix->n;
+    a->g.dim = ix->dim;
+    a->g.top = ix->top;
+    a->g.entry = ix->entry;
+    for (int h = 0; h < kMaxGroups; ++h) a->g.offsets[h] = ix->group_ptr[h];
+    a->queries = d_q;
+    a->nq = nq;
+    a->topk = d_topk;
+    a->queue = d_queue;
+    a->topk_default = r->topk;
+    a->queue_default = r->queue;
+    a->k_stride = k_stride;
+    a->cap = r->cap;
+    a->out = d_out;
+    a->stats = d_stats;
+    a->vis_bits = r->d_vis_bits;
+    a->vis_list = r->d_vis_list;
+    a->words_per_slot = r->words_per_slot;
+    a->list_cap = r->list_cap;
+    a->next_query = r->d_counter;
+    a->error = r->d_error;
+    a->l0_only = l0_only ? 1u : 0u;
+    return ARTEA_GPU_OK;
+}
+
+int launch_with(artea_gpu_router* r, SearchArgs a, bool persistent, uint32_t warps, cudaStream_t st) {
+    const bool exact = r->mode == ARTEA_GPU_MODE_EXACT;
+    KernelFn fn = pick_kernel(r->metric, exact, persistent);
+    if (!fn) return fail(ARTEA_GPU_EINVAL, "unknown metric");
+    if (a.nq == 0) return ARTEA_GPU_OK;
+    if (persistent) {
+        LaunchShape s;
+        if (int rc = persistent_shape(r, warps, &s)) return rc;
+        const uint32_t needed_ctas = (a.nq + warps - 1) / warps;
+        const uint32_t ctas = std::min(s.ctas, needed_ctas);
+        if (int rc = ensure_slots(r, ctas * warps)) return rc;
+        a.vis_bits = r->d_vis_bits;
+        a.vis_list = r->d_vis_list;
+        CUDA_TRY(cudaMemsetAsync(r->d_counter, 0, sizeof(uint32_t), st));
+        const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap) * warps;
+        fn<<<ctas, warps * 32, smem, st>>>(a);
+    } else {
+        if (int rc = ensure_slots(r, a.nq)) return rc;
+        a.vis_bits = r->d_vis_bits;
+        a.vis_list = r->d_vis_list;
+        const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap);
+        CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        fn<<<a.nq, 32, smem, st>>>(a);
+    }
+    r->launches++;
+    CUDA_TRY(cudaGetLastError());
+    return ARTEA_GPU_OK;
+}
+
+// Autotuner: warps per CTA for the persistent schedule, picked per
+// (dim, queue capacity) by timing each candidate on the first call's batch.
+int tuned_warps(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
+    if (r->want_warps) return static_cast<int>(r->want_warps);
+    const uint64_t key = (static_cast<uint64_t>(r->idx->dim) << 32) | r->cap;
+    auto it = r->tuned_warps.find(key);
+    if (it != r->tuned_warps.end()) return static_cast<int>(it->second);
+    static const uint32_t candidates[] = {1, 2, 4, 8};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best_ms = 1e30f;
+    uint32_t best = 4;
+    for (uint32_t w : candidates) {
+        LaunchShape s;
+        if (persistent_shape(r, w, &s) != ARTEA_GPU_OK) {
+            cudaGetLastError();
+            continue;
+        }
+        // One warm run, one timed run.
+        float ms = 0.f;
+        bool ok = true;
+        for (int rep = 0; rep < 2 && ok; ++rep) {
+            cudaEventRecord(e0, st);
+            ok = launch_with(r, a, true, w, st) == ARTEA_GPU_OK;
+            cudaEventRecord(e1, st);
+            ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
+        }
+        if (!ok) continue;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = w;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    r->tuned_warps[key] = best;
+    return static_cast<int>(best);
+}
+
+int check_kernel_error(artea_gpu_router* r) {
+    int h_err = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h_err, r->d_error, sizeof(int), cudaMemcpyDeviceToHost, r->stream));
+    CUDA_TRY(cudaStreamSynchronize(r->stream));
+    if (h_err != 0) {
+        cudaMemsetAsync(r->d_error, 0, sizeof(int), r->stream);
+        cudaStreamSynchronize(r->stream);
+        static const char* what[] = {"none", "neighbour id out of range", "iteration bound exceeded",
+                                     "queue capacity exceeded", "per-query topk/queue outside the router's limits"};
+        return fail(ARTEA_GPU_EKERNEL, std::string("kernel error: ") + (h_err > 0 && h_err < 5 ? what[h_err] : "?"));
+    }
+    return ARTEA_GPU_OK;
+}
+
+int run_device(artea_gpu_router* r, const float* d_q, uint32_t nq, const uint32_t* d_topk, const uint32_t* d_queue,
+               uint32_t k_stride, uint64_t* d_out, artea_gpu_query_stats* d_stats, bool l0_only, cudaStream_t st) {
+    DeviceGuard guard(r->idx->device);
+    if (k_stride == 0 && nq) return fail(ARTEA_GPU_EINVAL, "k_stride must be >= topk");
+    if (!d_topk && k_stride < r->topk) return fail(ARTEA_GPU_EINVAL, "k_stride must be >= topk");
+    if (nq && (!d_q || !d_out)) return fail(ARTEA_GPU_EINVAL, "null query or output buffer");
+    SearchArgs a;
+    fill_args(r, &a, d_q, nq, d_topk, d_queue, k_stride, d_out, d_stats, l0_only);
+    bool persistent = r->schedule == ARTEA_GPU_SCHEDULE_PERSISTENT;
+    if (r->schedule == ARTEA_GPU_SCHEDULE_AUTO) persistent = true;
+    uint32_t warps = 1;
+    if (persistent) warps = static_cast<uint32_t>(tuned_warps(r, a, st));
+    return launch_with(r, a, persistent, warps, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* artea_gpu_version(void) { return "artea-b200 0.1 (sm_100a)"; }
+
+const char* artea_gpu_last_error(void) { return artea_gpu::t_last_error.c_str(); }
+
+int artea_gpu_device_count(int* count) {
+    if (!count) return fail(ARTEA_GPU_EINVAL, "null count");
+    *count = 0;
+    const cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *count = 0;
+        return fail(ARTEA_GPU_ENODEV, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    return ARTEA_GPU_OK;
+}
+
+int artea_gpu_index_create(const artea_gpu_graph_desc* g, const float* vectors, uint32_t num_vectors, uint32_t dim,
+                           int device, artea_gpu_index** out) {
+    if (!g || !out) return fail(ARTEA_GPU_EINVAL, "null argument");
+    *out = nullptr;
+    if (dim == 0 || dim % 16 != 0) return fail(ARTEA_GPU_EINVAL, "dim must be a positive multiple of 16");
+    if (num_vectors < g->num_vertices) return fail(ARTEA_GPU_EINVAL, "fewer vectors than graph vertices");
+    if (num_vectors && !vectors) return fail(ARTEA_GPU_EINVAL, "null vectors");
+    if (int rc = artea_gpu_graph_validate(g)) return rc;
+    int ndev = 0;
+    if (artea_gpu_device_count(&ndev) != ARTEA_GPU_OK || device < 0 || device >= ndev)
+        return fail(ARTEA_GPU_ENODEV, "CUDA device " + std::to_string(device) + " not available");
+    DeviceGuard guard(device);
+
+    auto* ix = new artea_gpu_index();
+    ix->device = device;
+    ix->n = g->num_vertices;
+    ix->dim = dim;
+    const bool empty = g->num_vertices == 0 || g->top_level == kInvalidLevel;
+    ix->top = empty ? kInvalidLevel : g->top_level;
+    ix->entry = g->entry_point_vid;
+    ix->ul = g->ul_max_nbr_size;
+    ix->bl = g->bl_max_nbr_size;
+    auto cleanup = [&](int rc) {
+        artea_gpu_index_destroy(ix);
+        return rc;
+    };
+    const size_t nvec = static_cast<size_t>(std::max(num_vectors, 1u)) * dim;
+    if (int rc = dev_alloc(&ix->d_vecs, nvec)) return cleanup(rc);
+    if (num_vectors) {
+        if (cudaMemcpy(ix->d_vecs, vectors, sizeof(float) * static_cast<size_t>(num_vectors) * dim,
+                       cudaMemcpyHostToDevice) != cudaSuccess)
+            return cleanup(fail(ARTEA_GPU_ECUDA, "vector upload failed"));
+    }
+    ix->bytes += sizeof(float) * nvec;
+    if (!empty) {
+        if (int rc = dev_alloc(&ix->d_vinfo, ix->n)) return cleanup(rc);
+        if (cudaMemcpy(ix->d_vinfo, g->vertex_info, sizeof(uint2) * ix->n, cudaMemcpyHostToDevice) != cudaSuccess)
+            return cleanup(fail(ARTEA_GPU_ECUDA, "vertex table upload failed"));
+        const uint64_t nn = std::max<uint64_t>(g->num_neighbor_ids, 1);
+        if (int rc = dev_alloc(&ix->d_nbrs, nn)) return cleanup(rc);
+        if (g->num_neighbor_ids &&
+            cudaMemcpy(ix->d_nbrs, g->neighbor_ids, sizeof(uint32_t) * g->num_neighbor_ids, cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+            return cleanup(fail(ARTEA_GPU_ECUDA, "neighbour upload failed"));
+        uint64_t total = 0;
+        for (uint32_t h = 0; h <= ix->top; ++h) total += g->group_sizes[h] * (h + 1ull) + 1;
+        if (int rc = dev_alloc(&ix->d_offsets, total)) return cleanup(rc);
+        uint64_t at = 0;
+        for (uint32_t h = 0; h <= ix->top; ++h) {
+            const uint64_t cnt = g->group_sizes[h] * (h + 1ull) + 1;
+            if (cudaMemcpy(ix->d_offsets + at, g->group_offsets[h], sizeof(uint64_t) * cnt, cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+                return cleanup(fail(ARTEA_GPU_ECUDA, "offset upload failed"));
+            ix->group_ptr[h] = ix->d_offsets + at;
+            at += cnt;
+        }
+        ix->bytes += sizeof(uint2) * ix->n + sizeof(uint32_t) * nn + sizeof(uint64_t) * total;
+    }
+    *out = ix;
+    return ARTEA_GPU_OK;
+}
+
+int artea_gpu_index_create_from_hgra(const char* path, const float* vectors, uint32_t num_vectors, uint32_t dim,
+                                     int device, artea_gpu_index** out) {
+    if (!path || !out) return fail(ARTEA_GPU_EINVAL, "null argument");
+    artea_gpu_hgra_info info;
+    if (int rc = artea_gpu_hgra_probe(path, &info)) return rc;
+    std::vector<uint32_t> vinfo(2ull * info.num_vertices);
+    std::vector<uint64_t> offsets(info.num_offsets);
+    std::vector<uint32_t> nbrs(std::max<uint64_t>(info.num_neighbor_ids, 1));
+    if (int rc = artea_gpu_hgra_read(path, vinfo.data(), offsets.data(), nbrs.data())) return rc;
+    std::vector<const uint64_t*> gptr(info.num_groups);
+    uint64_t at = 0;
+    for (uint32_t h = 0; h < info.num_groups; ++h) {
+        gptr[h] = offsets.data() + at;
+        at += info.group_sizes[h] * (h + 1ull) + 1;
+    }
+    artea_gpu_graph_desc g;
+    g.num_vertices = info.num_vertices;
+    g.top_level = info.num_vertices == 0 ? kInvalidLevel : info.top_level;
+    g.ul_max_nbr_size = info.ul_max_nbr_size;
+    g.bl_max_nbr_size = info.bl_max_nbr_size;
+    g.entry_point_vid = info.entry_point_vid;
+    g.vertex_info = vinfo.data();
+    g.group_offsets = gptr.data();
+    g.group_sizes = info.group_sizes;
+    g.neighbor_ids = nbrs.data();
+    g.num_neighbor_ids = info.num_neighbor_ids;
+    return artea_gpu_index_create(&g, vectors, num_vectors, dim, device, out);
+}
+
+int artea_gpu_index_destroy(artea_gpu_index* ix) {
+    if (!ix) return ARTEA_GPU_OK;
+    DeviceGuard guard(ix->device);
+    dev_free(ix->d_vecs);
+    dev_free(ix->d_vinfo);
+    dev_free(ix->d_nbrs);
+    dev_free(ix->d_offsets);
+    delete ix;
+    return ARTEA_GPU_OK;
+}
+
+int artea_gpu_index_bytes(const artea_gpu_index* ix, uint64_t* bytes) {
+    if (!ix || !bytes) return fail(ARTEA_GPU_EINVAL, "null argument");
+    *bytes = ix->bytes;
+    return ARTEA_GPU_OK;
+}
+
+int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, const artea_gpu_router_opts* opts,
+                            artea_gpu_router** out) {
+    if (!ix || !out) return fail(ARTEA_GPU_EINVAL, "null argument");
+    *out = nullptr;
+    if (queue < topk) {
+        // hierarchical_graph_router.hpp:104-108
+        return fail(ARTEA_GPU_EINVAL, "candidate_queue_size (" + std::to_string(queue) + ") must be >= topk (" +
+                                          std::to_string(topk) + ")");
+    }
+    artea_gpu_router_opts o;
+    std::memset(&o, 0, sizeof(o));
+    if (opts) o = *opts;
+    if (o.metric < 0 || o.metric > 3) return fail(ARTEA_GPU_EINVAL, "unknown metric");
+    if (o.mode != ARTEA_GPU_MODE_EXACT && o.mode != ARTEA_GPU_MODE_FAST) return fail(ARTEA_GPU_EINVAL, "unknown mode");
+    if (o.schedule < 0 || o.schedule > 2) return fail(ARTEA_GPU_EINVAL, "unknown schedule");
+    if (o.warps_per_cta > 32) return fail(ARTEA_GPU_EINVAL, "warps_per_cta must be <= 32");
+    DeviceGuard guard(ix->device);
+    auto* r = new artea_gpu_router();
+    r->idx = ix;
+    r->topk = topk;
+    r->queue = queue;
+    r->max_queue = std::max(o.max_queue ? o.max_queue : queue, queue);
+    r->cap = std::max<uint32_t>(2u * r->max_queue, 2u);
+    r->max_batch = o.max_batch ? o.max_batch : 65536;
+    r->metric = o.metric;
+    r->mode = o.mode;
+    r->schedule = o.schedule;
+    r->want_warps = o.warps_per_cta;
+    r->want_ctas_per_sm = o.ctas_per_sm;
+    r->use_graphs = o.use_graphs != 0;
+    r->words_per_slot = ((static_cast<uint64_t>(ix->n) + 127) / 128) * 4;   // multiple of 4 words
+    r->list_cap = std::max<uint32_t>(std::min<uint32_t>(ix->n, 32768), 64);
+    auto cleanup = [&](int rc) {
+        artea_gpu_router_destroy(r);
+        return rc;
+    };
+    if (cudaDeviceGetAttribute(&r->num_sms, cudaDevAttrMultiProcessorCount, ix->device) != cudaSuccess)
+        return cleanup(fail(ARTEA_GPU_ECUDA, "cannot query SM count"));
+    if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(ARTEA_GPU_ECUDA, "cannot create stream"));
+    if (int rc = dev_alloc(&r->d_counter, 1)) return cleanup(rc);
+    if (int rc = dev_alloc(&r->d_error, 1)) return cleanup(rc);
+    if (cudaMemsetAsync(r->d_error, 0, sizeof(int), r->stream) != cudaSuccess)
+        return cleanup(fail(ARTEA_GPU_ECUDA, "memset failed"));
+    if (cudaStreamSynchronize(r->stream) != cudaSuccess) return cleanup(fail(ARTEA_GPU_ECUDA, "sync failed"));
+    *out = r;
+    return ARTEA_GPU_OK;
+}
+
+int artea_gpu_router_destroy(artea_gpu_router* r) {
+    if (!r) return ARTEA_GPU_OK;
+    DeviceGuard guard(r->idx->device);
+    if (r->stream) cudaStreamSynchronize(r->stream);
+    dev_free(r->d_vis_bits);
+    dev_free(r->d_vis_list);
+    dev_free(r->d_counter);
+    dev_free(r->d_error);
+    dev_free(r->d_queries);
+    dev_free(r->d_out);
+    dev_free(r->d_topk);
+    dev_free(r->d_queue);
+    dev_free(r->d_stats);
+    if (r->stream) cudaStreamDestroy(r->stream);
+    delete r;
+    return ARTEA_GPU_OK;
+}
+
+static int host_query(artea_gpu_router* r, const float* queries, uint32_t nq, const uint32_t* topk_pq,
+                      const uint32_t* queue_pq, uint32_t k_stride, uint64_t* out, artea_gpu_query_stats* stats,
+                      bool l0_only) {
+    if (!r) return fail(ARTEA_GPU_EINVAL, "null router");
+    if (nq == 0) return ARTEA_GPU_OK;
+    if (!queries || !out) return fail(ARTEA_GPU_EINVAL, "null query or output buffer");
+    if (nq > r->max_batch) return fail(ARTEA_GPU_EINVAL, "batch larger than the router's max_batch");
+    uint32_t kmax = r->topk;
+    if (topk_pq || queue_pq) {
+        kmax = 0;
+        for (uint32_t i = 0; i < nq; ++i) {
+            const uint32_t k = topk_pq ? topk_pq[i] : r->topk;
+            const uint32_t L = queue_pq ? queue_pq[i] : r->queue;
+            if (L < k) return fail(ARTEA_GPU_EINVAL, "query " + std::to_string(i) + ": queue < topk");
+            if (L > r->max_queue) return fail(ARTEA_GPU_EINVAL, "query " + std::to_string(i) + ": queue above max_queue");
+            kmax = std::max(kmax, k);
+        }
+    }
+    if (k_stride < kmax) return fail(ARTEA_GPU_EINVAL, "k_stride must be >= every topk");
+    DeviceGuard guard(r->idx->device);
+    if (int rc = ensure_stage(r, nq, k_stride)) return rc;
+    cudaStream_t st = r->stream;
+    CUDA_TRY(cudaMemcpyAsync(r->d_queries, queries, sizeof(float) * static_cast<size_t>(nq) * r->idx->dim,
+                             cudaMemcpyHostToDevice, st));
+    if (topk_pq) CUDA_TRY(cudaMemcpyAsync(r->d_topk, topk_pq, sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
+    if (queue_pq) CUDA_TRY(cudaMemcpyAsync(r->d_queue, queue_pq, sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
+    if (int rc = run_device(r, r->d_queries, nq, topk_pq ? r->d_topk : nullptr, queue_pq ? r->d_queue : nullptr,
+                            k_stride, r->d_out, stats ? r->d_stats : nullptr, l0_only, st))
+        return rc;
+    CUDA_TRY(cudaMemcpyAsync(out, r->d_out, sizeof(uint64_t) * static_cast<size_t>(nq) * k_stride,
+                             cudaMemcpyDeviceToHost, st));
+    if (stats)
+        CUDA_TRY(cudaMemcpyAsync(stats, r->d_stats, sizeof(artea_gpu_query_stats) * nq, cudaMemcpyDeviceToHost, st));
+    return check_kernel_error(r);
+}
+
+int artea_gpu_batch_query(artea_gpu_router* r, const float* queries, uint32_t nq, const uint32_t* topk_pq,
+                          const uint32_t* queue_pq, uint32_t k_stride, uint64_t* out, artea_gpu_query_stats* stats) {
+    return host_query(r, queries, nq, topk_pq, queue_pq, k_stride, out, stats, false);
+}
+
+int artea_gpu_batch_query_l0_only(artea_gpu_router* r, const float* queries, uint32_t nq, uint32_t k_stride,
+                                  uint64_t* out, artea_gpu_query_stats* stats) {
+    return host_query(r, queries, nq, nullptr, nullptr, k_stride, out, stats, true);
+}
+
+int artea_gpu_batch_query_device(artea_gpu_router* r, const float* d_q, uint32_t nq, const uint32_t* d_topk,
+                                 const uint32_t* d_queue, uint32_t k_stride, uint64_t* d_out,
+                                 artea_gpu_query_stats* d_stats, void* stream) {
+    if (!r) return fail(ARTEA_GPU_EINVAL, "null router");
+    if (nq > r->max_batch) return fail(ARTEA_GPU_EINVAL, "batch larger than the router's max_batch");
+    // NULL is the CUDA default stream, as in every CUDA API.
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return run_device(r, d_q, nq, d_topk, d_queue, k_stride, d_out, d_stats, false, st);
+}
+
+int artea_gpu_router_sync(artea_gpu_router* r) {
+    if (!r) return fail(ARTEA_GPU_EINVAL, "null router");
+    DeviceGuard guard(r->idx->device);
+    CUDA_TRY(cudaDeviceSynchronize());
+    return check_kernel_error(r);
+}
+
+int artea_gpu_router_launches(const artea_gpu_router* r, uint64_t* launches) {
+    if (!r || !launches) return fail(ARTEA_GPU_EINVAL, "null argument");
+    *launches = r->launches;
+    return ARTEA_GPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,658 @@
+// Device side of the B200 query path: one warp searches one query.
+//
+// Restates, on the GPU, hierarchical_graph_router.hpp:195-248 (_query with
+// RandomSeeding=false, enable_early_stop=false): entry point, greedy descent
+// on levels top..1 (detail/beam_loop.hpp:129-166), beam search on level 0
+// (detail/beam_loop.hpp:90-119) with StdCandidateQueue's rules
+// (router/data_structures/std_candidate_queue.hpp:358-513), top-k extraction
+// (std_candidate_queue.hpp:542-561).
+//
+// Data layout in HBM (uploaded once):
+//   vecs      N x D float32, D a multiple of 16, rows 64-byte aligned
+//   vinfo     N x {highest_level, local_vid} (uint2)
+//   offsets   per highest-level group h: N_h*(h+1)+1 uint64 CSR offsets
+//   nbrs      uint32 neighbour ids in CSR row order
+// Per search slot (one per resident warp):
+//   visited bitset (N bits) + visited list (ids set since the last clear)
+//
+// Shared memory per warp: the query row, the candidate queue (sorted array of
+// (dist, vid|explored) with room for 2L entries) and a candidate batch.
+#pragma once
+
+#include <cstdint>
+#include <cfloat>
+#include <cuda_runtime.h>
+
+#include "../../include/artea_gpu.h"
+
+namespace artea_gpu {
+
+constexpr uint32_t kFull = 0xffffffffu;
+constexpr uint32_t kExplored = 0x80000000u;
+constexpr uint32_t kVidMask = 0x7fffffffu;
+constexpr uint32_t kInvalidLevel = 0xffffffffu;
+constexpr uint32_t kCandBatch = 64;     // candidates evaluated per distance batch
+constexpr int kMaxGroups = 64;
+
+enum : int {
+    kErrNone = 0,
+    kErrBadVid = 1,        // an id >= N reached the kernel
+    kErrBound = 2,         // an iteration bound was exceeded
+    kErrQueue = 3,         // queue capacity exceeded (cannot happen for cap >= 2L)
+    kErrArgs = 4,          // per-query topk/queue outside the launch's limits
+};
+
+struct DeviceGraph {
+    const float* __restrict__ vecs;
+    const uint2* __restrict__ vinfo;
+    const uint32_t* __restrict__ nbrs;
+    uint32_t n;
+    uint32_t dim;
+    uint32_t top;      // kInvalidLevel when empty
+    uint32_t entry;
+    const uint64_t* offsets[kMaxGroups];
+};
+
+struct SearchArgs {
+    DeviceGraph g;
+    const float* __restrict__ queries;
+    uint32_t nq;
+    const uint32_t* __restrict__ topk;    // may be null
+    const uint32_t* __restrict__ queue;   // may be null
+    uint32_t topk_default;
+    uint32_t queue_default;
+    uint32_t k_stride;
+    uint32_t cap;                         // queue entries per warp (>= 2 * max queue)
+    uint64_t* __restrict__ out;
+    artea_gpu_query_stats* __restrict__ stats;   // may be null
+    uint32_t* __restrict__ vis_bits;      // slots x words_per_slot
+    uint32_t* __restrict__ vis_list;      // slots x list_cap
+    uint64_t words_per_slot;
+    uint32_t list_cap;
+    uint32_t* __restrict__ next_query;    // persistent schedule work counter
+    int* __restrict__ error;
+    uint32_t l0_only;
+};
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+__device__ __forceinline__ bool entry_less(float da, uint32_t va, float db, uint32_t vb) {
+    return da < db || (da == db && (va & kVidMask) < (vb & kVidMask));
+}
+
+__device__ __forceinline__ void set_error(int* error, int code) {
+    atomicCAS(error, 0, code);
+}
+
+// ---------------------------------------------------------------------------
+// Distances (subsystem d). 4 lanes per row, 8 rows per warp pass. Lane group
+// slot g in [0,4) owns AVX-512 lanes 4g..4g+3 of the reference's 16-lane
+// accumulation (utils/simd_distance.hpp:100-115): for chunk c it loads the
+// float4 at element 16c+4g and FMAs into four accumulators, so each
+// accumulator is exactly one reference lane's chain. The fold then follows
+// GCC's _mm512_reduce_add_ps tree: lanes (i, i+8) are warp lanes g and g^2,
+// lanes (i, i+4) are g and g^1, then (i, i^2) and lane0+lane1 inside a lane.
+// FAST mode folds each lane's four components first (warp order).
+// ---------------------------------------------------------------------------
+template <bool kExact>
+__device__ __forceinline__ float fold16(float a0, float a1, float a2, float a3) {
+    if (kExact) {
+        a0 = __fadd_rn(a0, __shfl_xor_sync(kFull, a0, 2));
+        a1 = __fadd_rn(a1, __shfl_xor_sync(kFull, a1, 2));
+        a2 = __fadd_rn(a2, __shfl_xor_sync(kFull, a2, 2));
+        a3 = __fadd_rn(a3, __shfl_xor_sync(kFull, a3, 2));
+        a0 = __fadd_rn(a0, __shfl_xor_sync(kFull, a0, 1));
+        a1 = __fadd_rn(a1, __shfl_xor_sync(kFull, a1, 1));
+        a2 = __fadd_rn(a2, __shfl_xor_sync(kFull, a2, 1));
+        a3 = __fadd_rn(a3, __shfl_xor_sync(kFull, a3, 1));
+        const float u0 = __fadd_rn(a0, a2);
+        const float u1 = __fadd_rn(a1, a3);
+        return __fadd_rn(u0, u1);
+    } else {
+        float s = (a0 + a1) + (a2 + a3);
+        s += __shfl_xor_sync(kFull, s, 1);
+        s += __shfl_xor_sync(kFull, s, 2);
+        return s;
+    }
+}
+
+__device__ __forceinline__ float4 ldg4(const float* p) {
+    return __ldg(reinterpret_cast<const float4*>(p));
+}
+
+// Squared norm of the query with the reference's lane structure (the nsq1
+// accumulator of utils/simd_distance.hpp:251-268), needed by cosine.
+template <bool kExact>
+__device__ float query_sqnorm(const float* __restrict__ q, uint32_t dim) {
+    const int g = lane_id() & 3;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    for (uint32_t c = 0; c < dim; c += 16) {
+        const float4 v = *reinterpret_cast<const float4*>(q + c + 4 * g);
+        a0 = fmaf(v.x, v.x, a0); a1 = fmaf(v.y, v.y, a1);
+        a2 = fmaf(v.z, v.z, a2); a3 = fmaf(v.w, v.w, a3);
+    }
+    return fold16<kExact>(a0, a1, a2, a3);
+}
+
+// Distances for cnt candidates (ids in cvid, shared memory) into cdist.
+// Per pass each lane issues up to kBlock float4 loads of its row segment
+// before any arithmetic, so a D=128 row costs one memory round trip.
+constexpr int kBlock = 8;
+
+template <int kMetric>
+__device__ __forceinline__ void accumulate(const float4 x, const float4 y, float& a0, float& a1, float& a2,
+                                           float& a3, float& b0, float& b1, float& b2, float& b3) {
+    if (kMetric == ARTEA_GPU_EUCLIDEAN_SQR || kMetric == ARTEA_GPU_EUCLIDEAN) {
+        const float d0 = __fsub_rn(y.x, x.x), d1 = __fsub_rn(y.y, x.y);
+        const float d2 = __fsub_rn(y.z, x.z), d3 = __fsub_rn(y.w, x.w);
+        a0 = fmaf(d0, d0, a0); a1 = fmaf(d1, d1, a1);
+        a2 = fmaf(d2, d2, a2); a3 = fmaf(d3, d3, a3);
+    } else {
+        a0 = fmaf(y.x, x.x, a0); a1 = fmaf(y.y, x.y, a1);
+        a2 = fmaf(y.z, x.z, a2); a3 = fmaf(y.w, x.w, a3);
+        if (kMetric == ARTEA_GPU_COSINE) {
+            b0 = fmaf(x.x, x.x, b0); b1 = fmaf(x.y, x.y, b1);
+            b2 = fmaf(x.z, x.z, b2); b3 = fmaf(x.w, x.w, b3);
+        }
+    }
+}
+
+template <int kMetric, bool kExact>
+__device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ q, float qsq,
+                                const uint32_t* cvid, float* cdist, uint32_t cnt) {
+    const int lane = lane_id();
+    const int r = lane >> 2;
+    const int gi = lane & 3;
+    const uint32_t dim = g.dim;
+    const uint32_t nchunks = dim >> 4;
+    for (uint32_t p = 0; p < cnt; p += 8) {
+        const uint32_t idx = p + r;
+        const bool valid = idx < cnt;
+        const uint32_t vid = valid ? cvid[idx] : 0u;
+        const float* row = g.vecs + static_cast<size_t>(vid) * dim + 4 * gi;
+        const float* qq = q + 4 * gi;
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;   // L2: diff^2; dot/cos: q*x
+        float b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f;   // cos: x*x
+        for (uint32_t cb = 0; cb < nchunks; cb += kBlock) {
+            float4 x[kBlock];
+#pragma unroll
+            for (int k = 0; k < kBlock; ++k) {
+                x[k] = (valid && cb + k < nchunks) ? ldg4(row + 16 * (cb + k)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int k = 0; k < kBlock; ++k) {
+                if (cb + k < nchunks) {
+                    const float4 y = *reinterpret_cast<const float4*>(qq + 16 * (cb + k));
+                    accumulate<kMetric>(x[k], y, a0, a1, a2, a3, b0, b1, b2, b3);
+                }
+            }
+        }
+        float res = fold16<kExact>(a0, a1, a2, a3);
+        if (kMetric == ARTEA_GPU_EUCLIDEAN) {
+            res = __fsqrt_rn(res);
+        } else if (kMetric == ARTEA_GPU_DOT) {
+            res = -res;
+        } else if (kMetric == ARTEA_GPU_COSINE) {
+            const float xsq = fold16<kExact>(b0, b1, b2, b3);
+            // utils/simd_distance.hpp:263-274
+            const float denom = __fsqrt_rn(__fmul_rn(qsq, xsq));
+            res = denom > 0.0f ? __fsub_rn(1.0f, __fdiv_rn(res, denom)) : 1.0f;
+        }
+        if (valid && gi == 0) cdist[idx] = res;
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// Visited set (subsystem c): per-slot bitset in HBM; atomicOr gives
+// test_and_set (containers/version_tag_table.hpp:128-132). Every id set is
+// appended to the slot's list so clear() (a version bump in the reference,
+// version_tag_table.hpp:142-148) only zeroes the words it touched; if the list
+// overflows, the whole bitset is zeroed instead.
+// ---------------------------------------------------------------------------
+struct Visited {
+    uint32_t* bits;
+    uint32_t* list;
+    uint32_t list_n;
+    uint32_t list_cap;
+    uint64_t words;
+    bool spilled;
+    uint32_t spills;
+};
+
+__device__ __forceinline__ void visited_record(Visited& vs, uint32_t vid, bool is_new) {
+    const int lane = lane_id();
+    const uint32_t b = __ballot_sync(kFull, is_new);
+    const uint32_t pos = vs.list_n + __popc(b & ((1u << lane) - 1u));
+    if (is_new) {
+        if (pos < vs.list_cap) vs.list[pos] = vid;
+    }
+    const uint32_t total = vs.list_n + __popc(b);
+    if (total > vs.list_cap) vs.spilled = true;
+    vs.list_n = min(total, vs.list_cap);
+}
+
+// set(): mark one id (all lanes call with the same vid).
+__device__ __forceinline__ void visited_set(Visited& vs, uint32_t vid) {
+    const int lane = lane_id();
+    bool is_new = false;
+    if (lane == 0) {
+        const uint32_t old = atomicOr(vs.bits + (vid >> 5), 1u << (vid & 31));
+        is_new = !(old & (1u << (vid & 31)));
+    }
+    visited_record(vs, vid, is_new);
+}
+
+__device__ void visited_clear(Visited& vs) {
+    const int lane = lane_id();
+    __syncwarp();
+    if (vs.spilled) {
+        uint4* w4 = reinterpret_cast<uint4*>(vs.bits);
+        const uint64_t n4 = vs.words / 4;
+        for (uint64_t i = lane; i < n4; i += 32) w4[i] = make_uint4(0, 0, 0, 0);
+        vs.spills++;
+    } else {
+        for (uint32_t i = lane; i < vs.list_n; i += 32) vs.bits[vs.list[i] >> 5] = 0u;
+    }
+    vs.list_n = 0;
+    vs.spilled = false;
+    __threadfence_block();
+    __syncwarp();
+}
+
+// Collect the not-yet-visited ids of row[0, len) (CSR order, first occurrence
+// wins, marking them visited) into cvid[0, *cnt). Returns false on a bad id.
+// Processes at most kCandBatch new ids; *consumed reports how far it got.
+__device__ bool collect_unvisited(const DeviceGraph& g, Visited& vs, const uint32_t* __restrict__ row,
+                                  uint32_t len, uint32_t start, uint32_t* cvid, uint32_t* cnt,
+                                  uint32_t* consumed, int* error) {
+    const int lane = lane_id();
+    uint32_t c = 0;
+    uint32_t i = start;
+    bool ok = true;
+    while (i < len && c + 32 <= kCandBatch) {
+        const uint32_t idx = i + lane;
+        const bool act = idx < len;
+        uint32_t vid = act ? __ldg(row + idx) : 0xffffffffu;
+        if (act && vid >= g.n) {
+            set_error(error, kErrBadVid);
+            ok = false;
+        }
+        const uint32_t peers = __match_any_sync(kFull, vid);
+        const bool first = act && ((peers & ((1u << lane) - 1u)) == 0) && vid < g.n;
+        bool is_new = false;
+        if (first) {
+            const uint32_t mask = 1u << (vid & 31);
+            const uint32_t old = atomicOr(vs.bits + (vid >> 5), mask);
+            is_new = !(old & mask);
+        }
+        visited_record(vs, vid, is_new);
+        const uint32_t b = __ballot_sync(kFull, is_new);
+        if (is_new) cvid[c + __popc(b & ((1u << lane) - 1u))] = vid;
+        c += __popc(b);
+        i += 32;
+    }
+    __syncwarp();
+    *cnt = c;
+    *consumed = min(i, len);
+    return __all_sync(kFull, ok);
+}
+
+// ---------------------------------------------------------------------------
+// Candidate queue (subsystem b). Sorted ascending by (dist, vid) in shared
+// memory; bit 31 of the vid word marks "explored". T = the first min(n, L)
+// entries. Entries past L that tie the worst distance lb are entries the
+// reference evicted from its top-L heap but still holds in its unexplored
+// heap; they stay expandable until lb drops. Any entry worse than lb is dead
+// and trimmed. At most L entries can tie lb, so 2L slots always suffice.
+// ---------------------------------------------------------------------------
+struct Queue {
+    float* d;
+    uint32_t* v;
+    uint32_t n;
+    uint32_t L;
+    uint32_t cap;
+    uint32_t hint;   // no unexplored entry before this index
+    float lb;        // d[L-1] once n >= L
+};
+
+__device__ __forceinline__ uint32_t queue_lower_bound(const Queue& q, float d, uint32_t v) {
+    const int lane = lane_id();
+    uint32_t lo = 0, hi = q.n;
+    while (hi - lo > 32) {
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t idx = lo + lane * step;
+        const bool less = idx < hi && entry_less(q.d[idx], q.v[idx], d, v);
+        const int c = __popc(__ballot_sync(kFull, less));
+        const uint32_t new_lo = c == 0 ? lo : lo + (c - 1) * step + 1;
+        const uint32_t new_hi = min(hi, lo + c * step);
+        lo = new_lo;
+        hi = new_hi;
+    }
+    const uint32_t idx = lo + lane;
+    const bool less = idx < hi && entry_less(q.d[idx], q.v[idx], d, v);
+    return lo + __popc(__ballot_sync(kFull, less));
+}
+
+// Insert (d, v); the caller has already applied try_push's rejection test.
+__device__ __forceinline__ bool queue_insert(Queue& q, float d, uint32_t v, int* error) {
+    const int lane = lane_id();
+    if (q.n >= q.cap) {
+        set_error(error, kErrQueue);
+        return false;
+    }
+    const uint32_t pos = queue_lower_bound(q, d, v);
+    for (int end = static_cast<int>(q.n); end > static_cast<int>(pos); end -= 32) {
+        const int s = max(static_cast<int>(pos), end - 32);
+        const int idx = s + lane;
+        const bool act = idx < end;
+        float dd = 0.f;
+        uint32_t vv = 0;
+        if (act) { dd = q.d[idx]; vv = q.v[idx]; }
+        __syncwarp();
+        if (act) { q.d[idx + 1] = dd; q.v[idx + 1] = vv; }
+        __syncwarp();
+    }
+    if (lane == 0) { q.d[pos] = d; q.v[pos] = v & kVidMask; }
+    __syncwarp();
+    q.n++;
+    if (pos < q.hint) q.hint = pos;
+    if (q.n >= q.L) {
+        q.lb = q.d[q.L - 1];
+        if (q.n > q.L) {
+            uint32_t newn = q.n;
+            for (uint32_t base = q.L; base < q.n; base += 32) {
+                const uint32_t idx = base + lane;
+                const bool dead = idx < q.n && q.d[idx] > q.lb;
+                const uint32_t b = __ballot_sync(kFull, dead);
+                if (b) { newn = base + __ffs(b) - 1; break; }
+            }
+            q.n = newn;
+        }
+    }
+    return true;
+}
+
+// pop_best_unexplored_entry + should_terminate (std_candidate_queue.hpp:398-406,
+// 503-513): the first unexplored entry in order, or -1 when the reference's
+// unexplored heap holds nothing at distance <= lb.
+__device__ __forceinline__ int queue_pop(Queue& q) {
+    const int lane = lane_id();
+    for (uint32_t base = q.hint; base < q.n; base += 32) {
+        const uint32_t idx = base + lane;
+        const bool un = idx < q.n && !(q.v[idx] & kExplored);
+        const uint32_t b = __ballot_sync(kFull, un);
+        if (b) {
+            const uint32_t p = base + __ffs(b) - 1;
+            if (lane == 0) q.v[p] |= kExplored;
+            __syncwarp();
+            q.hint = p + 1;
+            return static_cast<int>(p);
+        }
+    }
+    q.hint = q.n;
+    return -1;
+}
+
+// try_push for a batch, in candidate order (std_candidate_queue.hpp:358-388):
+// reject when T is full and d >= lb, else insert.
+__device__ __forceinline__ void queue_push_batch_exact(Queue& q, const uint32_t* cvid, const float* cdist,
+                                                       uint32_t cnt, int* error) {
+    const int lane = lane_id();
+    uint32_t i = 0;
+    while (i < cnt) {
+        uint32_t j;
+        if (q.n < q.L) {
+            j = i;
+        } else {
+            j = 0xffffffffu;
+            for (uint32_t base = i; base < cnt; base += 32) {
+                const uint32_t idx = base + lane;
+                const bool acc = idx < cnt && cdist[idx] < q.lb;
+                const uint32_t b = __ballot_sync(kFull, acc);
+                if (b) { j = base + __ffs(b) - 1; break; }
+            }
+            if (j == 0xffffffffu) break;
+        }
+        if (!queue_insert(q, cdist[j], cvid[j], error)) return;
+        i = j + 1;
+    }
+}
+
+// FAST-mode merge: every candidate better than the current lb (or any while T
+// is not full) is inserted in one pass per candidate without re-testing
+// against the lb it lowers; ties are then ordered by vid.
+__device__ __forceinline__ void queue_push_batch_fast(Queue& q, const uint32_t* cvid, const float* cdist,
+                                                      uint32_t cnt, int* error) {
+    const float lb0 = q.n >= q.L ? q.lb : FLT_MAX;
+    for (uint32_t j = 0; j < cnt; ++j) {
+        const float d = cdist[j];
+        if (q.n >= q.L && !(d < q.lb)) continue;
+        if (!(d < lb0) && q.n >= q.L) continue;
+        if (!queue_insert(q, d, cvid[j], error)) return;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row lookup: fetch_level_nbrs (index/compact_structure/hierarchical_graph.hpp:99-108).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ const uint32_t* level_row(const DeviceGraph& g, uint32_t vid, uint32_t level,
+                                                     uint32_t* len) {
+    const uint2 info = __ldg(g.vinfo + vid);
+    const uint32_t hl = info.x;
+    if (hl == kInvalidLevel || hl < level || hl >= kMaxGroups) {
+        *len = 0;
+        return g.nbrs;
+    }
+    const uint64_t row = static_cast<uint64_t>(info.y) * (hl + 1ull) + (hl - level);
+    const uint64_t* off = g.offsets[hl];
+    const uint64_t b = __ldg(reinterpret_cast<const unsigned long long*>(off + row));
+    const uint64_t e = __ldg(reinterpret_cast<const unsigned long long*>(off + row + 1));
+    *len = static_cast<uint32_t>(e - b);
+    return g.nbrs + b;
+}
+
+struct Counters {
+    uint32_t dist_evals, upper_rows, upper_row_ids, l0_rows, l0_row_ids, upper_dist_evals;
+};
+
+// ---------------------------------------------------------------------------
+// One query (hierarchical_graph_router.hpp:195-248; query_l0_only :258-286).
+// ---------------------------------------------------------------------------
+template <int kMetric, bool kExact>
+__device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, float* smem_q, float* qd, uint32_t* qv,
+                           uint32_t* cvid, float* cdist) {
+    const int lane = lane_id();
+    const DeviceGraph& g = a.g;
+    const uint32_t dim = g.dim;
+    const uint32_t topk = a.topk ? a.topk[qi] : a.topk_default;
+    const uint32_t L = a.queue ? a.queue[qi] : a.queue_default;
+    uint64_t* out = a.out + static_cast<size_t>(qi) * a.k_stride;
+    constexpr uint64_t kInvalidWord = (static_cast<uint64_t>(0x7f7fffffu) << 32) | kVidMask;
+
+    if (topk > a.k_stride || L < topk || 2ull * L > a.cap) {
+        set_error(a.error, kErrArgs);
+        for (uint32_t i = lane; i < a.k_stride; i += 32) out[i] = kInvalidWord;
+        return;
+    }
+
+    Counters ct = {};
+    uint32_t nres = 0;
+    Visited vs;
+    vs.bits = a.vis_bits + static_cast<size_t>(slot) * a.words_per_slot;
+    vs.list = a.vis_list + static_cast<size_t>(slot) * a.list_cap;
+    vs.list_n = 0;
+    vs.list_cap = a.list_cap;
+    vs.words = a.words_per_slot;
+    vs.spilled = false;
+    vs.spills = 0;
+
+    if (g.n != 0 && g.top != kInvalidLevel && L > 0) {
+        // Stage the query row in shared memory.
+        const float4* src = reinterpret_cast<const float4*>(a.queries + static_cast<size_t>(qi) * dim);
+        float4* dst = reinterpret_cast<float4*>(smem_q);
+        for (uint32_t i = lane; i < dim / 4; i += 32) dst[i] = __ldg(src + i);
+        __syncwarp();
+        const float qsq = (kMetric == ARTEA_GPU_COSINE) ? query_sqnorm<kExact>(smem_q, dim) : 0.f;
+
+        // Entry point distance (hierarchical_graph_router.hpp:209-211).
+        uint32_t cur = g.entry;
+        if (lane == 0) cvid[0] = cur;
+        __syncwarp();
+        batch_distances<kMetric, kExact>(g, smem_q, qsq, cvid, cdist, 1);
+        float cur_d = cdist[0];
+        ct.dist_evals = 1;
+
+        // Greedy descent, levels top..1 (hierarchical_graph_router.hpp:228-236).
+        if (!a.l0_only) {
+            for (uint32_t h = g.top; h >= 1; --h) {
+                visited_set(vs, cur);
+                for (uint32_t hop = 0;; ++hop) {
+                    if (hop > g.n) { set_error(a.error, kErrBound); break; }
+                    uint32_t len;
+                    const uint32_t* row = level_row(g, cur, h, &len);
+                    ct.upper_rows++;
+                    ct.upper_row_ids += len;
+                    float best_d = cur_d;
+                    uint32_t best_v = cur;
+                    uint32_t pos = 0;
+                    while (pos < len) {
+                        uint32_t cnt, consumed;
+                        collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error);
+                        pos = consumed;
+                        if (cnt == 0) continue;
+                        batch_distances<kMetric, kExact>(g, smem_q, qsq, cvid, cdist, cnt);
+                        ct.dist_evals += cnt;
+                        ct.upper_dist_evals += cnt;
+                        // First strict improvement in row order (beam_loop.hpp:153-160).
+                        float md = INFINITY;
+                        uint32_t mi = 0xffffffffu;
+                        for (uint32_t i = lane; i < cnt; i += 32) {
+                            const float d = cdist[i];
+                            if (d < md) { md = d; mi = i; }
+                        }
+                        for (int off = 16; off > 0; off >>= 1) {
+                            const float od = __shfl_xor_sync(kFull, md, off);
+                            const uint32_t oi = __shfl_xor_sync(kFull, mi, off);
+                            if (od < md || (od == md && oi < mi)) { md = od; mi = oi; }
+                        }
+                        if (md < best_d) {
+                            best_d = md;
+                            best_v = cvid[mi];
+                        }
+                        __syncwarp();
+                    }
+                    if (best_v == cur) break;
+                    cur = best_v;
+                    cur_d = best_d;
+                }
+                visited_clear(vs);
+            }
+        }
+
+        // Level-0 beam search (single_layer_router.hpp:145-163, beam_loop.hpp:90-119).
+        Queue q;
+        q.d = qd;
+        q.v = qv;
+        q.n = 0;
+        q.L = L;
+        q.cap = a.cap;
+        q.hint = 0;
+        q.lb = FLT_MAX;
+        queue_insert(q, cur_d, cur, a.error);
+        visited_set(vs, cur);
+        for (uint32_t it = 0;; ++it) {
+            if (it > g.n) { set_error(a.error, kErrBound); break; }
+            const int p = queue_pop(q);
+            if (p < 0) break;
+            const uint32_t v = q.v[p] & kVidMask;
+            if (v == kVidMask) break;   // CandidateEntry::is_invalid
+            uint32_t len;
+            const uint32_t* row = level_row(g, v, 0, &len);
+            ct.l0_rows++;
+            ct.l0_row_ids += len;
+            uint32_t pos = 0;
+            while (pos < len) {
+                uint32_t cnt, consumed;
+                collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error);
+                pos = consumed;
+                if (cnt == 0) continue;
+                batch_distances<kMetric, kExact>(g, smem_q, qsq, cvid, cdist, cnt);
+                ct.dist_evals += cnt;
+                if (kExact) queue_push_batch_exact(q, cvid, cdist, cnt, a.error);
+                else queue_push_batch_fast(q, cvid, cdist, cnt, a.error);
+                __syncwarp();
+            }
+        }
+        visited_clear(vs);
+
+        // extract_results(min(topk, |T|)) (std_candidate_queue.hpp:542-561).
+        const uint32_t tsize = min(q.n, q.L);
+        nres = min(topk, tsize);
+        for (uint32_t i = lane; i < a.k_stride; i += 32) {
+            uint64_t w = kInvalidWord;
+            if (i < nres) {
+                w = (static_cast<uint64_t>(__float_as_uint(qd[i])) << 32) | (qv[i] & kVidMask);
+            }
+            out[i] = w;
+        }
+    } else {
+        for (uint32_t i = lane; i < a.k_stride; i += 32) out[i] = kInvalidWord;
+    }
+
+    if (a.stats && lane == 0) {
+        artea_gpu_query_stats s;
+        s.dist_evals = ct.dist_evals;
+        s.upper_rows = ct.upper_rows;
+        s.upper_row_ids = ct.upper_row_ids;
+        s.l0_rows = ct.l0_rows;
+        s.l0_row_ids = ct.l0_row_ids;
+        s.upper_dist_evals = ct.upper_dist_evals;
+        s.results = nres;
+        s.visited_spills = vs.spills;
+        a.stats[qi] = s;
+    }
+    __syncwarp();
+}
+
+// Shared memory floats per warp for a launch.
+__host__ __device__ inline uint32_t warp_smem_words(uint32_t dim, uint32_t cap) {
+    return dim + 2 * cap + 2 * kCandBatch;
+}
+
+// Plain schedule: one CTA of one warp per query; slot = query index.
+template <int kMetric, bool kExact>
+__global__ void __launch_bounds__(32) search_plain_kernel(SearchArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    const uint32_t qi = blockIdx.x;
+    if (qi >= a.nq) return;
+    float* smem_q = smem;
+    float* qd = smem_q + a.g.dim;
+    uint32_t* qv = reinterpret_cast<uint32_t*>(qd + a.cap);
+    uint32_t* cvid = qv + a.cap;
+    float* cdist = reinterpret_cast<float*>(cvid + kCandBatch);
+    search_one<kMetric, kExact>(a, qi, qi, smem_q, qd, qv, cvid, cdist);
+}
+
+// Persistent schedule: warps pull query indices from a shared counter.
+template <int kMetric, bool kExact>
+__global__ void search_persistent_kernel(SearchArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    const int warp = threadIdx.x >> 5;
+    const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
+    float* base = smem + static_cast<size_t>(warp) * warp_smem_words(a.g.dim, a.cap);
+    float* smem_q = base;
+    float* qd = smem_q + a.g.dim;
+    uint32_t* qv = reinterpret_cast<uint32_t*>(qd + a.cap);
+    uint32_t* cvid = qv + a.cap;
+    float* cdist = reinterpret_cast<float*>(cvid + kCandBatch);
+    for (;;) {
+        uint32_t qi = 0;
+        if (lane_id() == 0) qi = atomicAdd(a.next_query, 1u);
+        qi = __shfl_sync(kFull, qi, 0);
+        if (qi >= a.nq) break;
+        search_one<kMetric, kExact>(a, qi, slot, smem_q, qd, qv, cvid, cdist);
+    }
+}
+
+}  // namespace artea_gpu

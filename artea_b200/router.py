@@ -1,0 +1,247 @@
+"""Python mirror of the reference router surface, backed by the B200 kernels.
+
+``HierarchicalGraphRouter`` follows hierarchical_graph_router_t<Metric, Dim>
+(router/hierarchical_graph_router.hpp:66-430): constructed from the base
+vectors, a metric, topk and the candidate queue size (raising like the
+reference's ARTEA_ERROR when queue < topk), ``initialize()``, then
+``batch_query(query_vecs, graph)`` returning the knn_results_t layout: nq*k
+8-byte CandidateEntry words, row-major, invalid-filled. The graph is uploaded
+on first use and kept device resident, keyed by the graph object.
+
+There is no CPU path: every call goes through libartea_gpu.so.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import weakref
+from typing import Optional
+
+import numpy as np
+
+from . import _native as nat
+from .graph import CompactHierarchicalGraph
+
+METRICS = {
+    "euclidean_sqr": nat.METRIC_EUCLIDEAN_SQR,
+    "l2sq": nat.METRIC_EUCLIDEAN_SQR,
+    "euclidean": nat.METRIC_EUCLIDEAN,
+    "cosine": nat.METRIC_COSINE,
+    "dot": nat.METRIC_DOT,
+}
+MODES = {"exact": nat.MODE_EXACT, "fast": nat.MODE_FAST}
+SCHEDULES = {"auto": nat.SCHEDULE_AUTO, "plain": nat.SCHEDULE_PLAIN, "persistent": nat.SCHEDULE_PERSISTENT}
+
+INVALID_WORD = np.uint64((0x7F7FFFFF << 32) | 0x7FFFFFFF)
+
+
+def entry_vids(words: np.ndarray) -> np.ndarray:
+    """CandidateEntry::get_vid (candidate_entry.hpp:115-118)."""
+    return (np.asarray(words, dtype=np.uint64) & np.uint64(0x7FFFFFFF)).astype(np.uint32)
+
+
+def entry_dists(words: np.ndarray) -> np.ndarray:
+    """CandidateEntry::get_distance."""
+    return (np.asarray(words, dtype=np.uint64) >> np.uint64(32)).astype(np.uint32).view(np.float32)
+
+
+def entry_is_invalid(words: np.ndarray) -> np.ndarray:
+    """CandidateEntry::is_invalid (candidate_entry.hpp:122-125)."""
+    return entry_vids(words) == 0x7FFFFFFF
+
+
+def metric_code(metric) -> int:
+    if isinstance(metric, str):
+        return METRICS[metric.lower()]
+    return int(metric)
+
+
+class DeviceIndex:
+    """A compact graph plus its FP32 vectors, uploaded once to one GPU."""
+
+    def __init__(self, graph: CompactHierarchicalGraph, base_vecs: np.ndarray, device: int = 0):
+        base = np.ascontiguousarray(base_vecs, dtype=np.float32)
+        if base.ndim != 2:
+            raise ValueError("base_vecs must be a 2-D array")
+        self.num_vectors, self.dim = base.shape
+        self.device = device
+        d = graph.desc()
+        h = ctypes.c_void_p()
+        nat.check(nat.lib().artea_gpu_index_create(ctypes.byref(d), nat.ptr(base), self.num_vectors, self.dim,
+                                                   device, ctypes.byref(h)))
+        self._h = h
+
+    @classmethod
+    def from_hgra(cls, path: str, base_vecs: np.ndarray, device: int = 0) -> "DeviceIndex":
+        self = cls.__new__(cls)
+        base = np.ascontiguousarray(base_vecs, dtype=np.float32)
+        self.num_vectors, self.dim = base.shape
+        self.device = device
+        h = ctypes.c_void_p()
+        import os
+        nat.check(nat.lib().artea_gpu_index_create_from_hgra(os.fsencode(path), nat.ptr(base), self.num_vectors,
+                                                             self.dim, device, ctypes.byref(h)))
+        self._h = h
+        return self
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if self._h is None:
+            raise RuntimeError("index is closed")
+        return self._h
+
+    def nbytes(self) -> int:
+        b = ctypes.c_uint64()
+        nat.check(nat.lib().artea_gpu_index_bytes(self.handle, ctypes.byref(b)))
+        return int(b.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            nat.lib().artea_gpu_index_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuRouter:
+    """A router handle bound to one DeviceIndex (artea_gpu_router_create)."""
+
+    def __init__(self, index: DeviceIndex, metric, topk: int, candidate_queue_size: int, mode: str = "exact",
+                 schedule: str = "auto", warps_per_cta: int = 0, ctas_per_sm: int = 0, max_batch: int = 0,
+                 max_queue: int = 0):
+        opts = nat.RouterOpts()
+        opts.metric = metric_code(metric)
+        opts.mode = MODES[mode] if isinstance(mode, str) else int(mode)
+        opts.schedule = SCHEDULES[schedule] if isinstance(schedule, str) else int(schedule)
+        opts.warps_per_cta = warps_per_cta
+        opts.ctas_per_sm = ctas_per_sm
+        opts.max_batch = max_batch
+        opts.max_queue = max_queue
+        h = ctypes.c_void_p()
+        nat.check(nat.lib().artea_gpu_router_create(index.handle, topk, candidate_queue_size, ctypes.byref(opts),
+                                                    ctypes.byref(h)))
+        self.index = index
+        self.topk = topk
+        self.queue = candidate_queue_size
+        self._h = h
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def batch_query(self, queries: np.ndarray, topk: Optional[np.ndarray] = None, queue: Optional[np.ndarray] = None,
+                    k_stride: Optional[int] = None, stats: bool = False, l0_only: bool = False):
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        if q.ndim != 2 or q.shape[1] != self.index.dim:
+            raise ValueError(f"queries must be (nq, {self.index.dim})")
+        nq = q.shape[0]
+        tk = None if topk is None else np.ascontiguousarray(topk, dtype=np.uint32)
+        qu = None if queue is None else np.ascontiguousarray(queue, dtype=np.uint32)
+        if k_stride is None:
+            k_stride = int(tk.max()) if tk is not None and tk.size else self.topk
+        out = np.empty((nq, max(k_stride, 0)), dtype=np.uint64)
+        st = (nat.QueryStats * max(nq, 1))() if stats else None
+        L = nat.lib()
+        if l0_only:
+            if tk is not None or qu is not None:
+                raise ValueError("l0_only takes the router's topk and queue")
+            rc = L.artea_gpu_batch_query_l0_only(self._h, nat.ptr(q), nq, k_stride, nat.ptr(out),
+                                                 ctypes.cast(st, ctypes.c_void_p) if st is not None else None)
+        else:
+            rc = L.artea_gpu_batch_query(self._h, nat.ptr(q), nq, nat.ptr(tk), nat.ptr(qu), k_stride,
+                                         nat.ptr(out), ctypes.cast(st, ctypes.c_void_p) if st is not None else None)
+        nat.check(rc)
+        if stats:
+            arr = np.ctypeslib.as_array(st)[:nq]
+            return out, np.array(arr.tolist(), dtype=np.uint32).reshape(nq, 8)
+        return out
+
+    def batch_query_device(self, d_queries, nq: int, k_stride: int, d_out, d_topk=None, d_queue=None, d_stats=None,
+                           stream: int = 0) -> None:
+        """Enqueue on device buffers (torch tensors or raw addresses); no sync."""
+        nat.check(nat.lib().artea_gpu_batch_query_device(self._h, nat.ptr(d_queries), nq, nat.ptr(d_topk),
+                                                         nat.ptr(d_queue), k_stride, nat.ptr(d_out),
+                                                         nat.ptr(d_stats), ctypes.c_void_p(stream or None)))
+
+    def sync(self) -> None:
+        nat.check(nat.lib().artea_gpu_router_sync(self._h))
+
+    def launches(self) -> int:
+        n = ctypes.c_uint64()
+        nat.check(nat.lib().artea_gpu_router_launches(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            nat.lib().artea_gpu_router_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HierarchicalGraphRouter:
+    """Drop-in for hierarchical_graph_router_t<Metric, Dim>.
+
+    ``base_vecs`` is held by reference, as the reference router holds a const
+    reference (router/vector_router.hpp:46, 63-69). ``batch_query`` takes the
+    graph per call; the first call with a graph uploads it (with the vectors)
+    and later calls reuse the device copy.
+    """
+
+    def __init__(self, base_vecs: np.ndarray, metric, topk: int, candidate_queue_size: int = 16,
+                 mode: str = "exact", schedule: str = "auto", device: int = 0, **router_opts):
+        if candidate_queue_size < topk:
+            # hierarchical_graph_router.hpp:104-108 (ARTEA_ERROR throws std::runtime_error)
+            raise RuntimeError(f"candidate_queue_size ({candidate_queue_size}) must be >= topk ({topk})")
+        self.base_vecs = base_vecs
+        self.metric = metric_code(metric)
+        self.topk = int(topk)
+        self.candidate_queue_size = int(candidate_queue_size)
+        self.mode = mode
+        self.schedule = schedule
+        self.device = device
+        self.router_opts = router_opts
+        self._cache = {}
+
+    def initialize(self) -> None:
+        """hierarchical_graph_router.hpp:114-117; device state is created lazily per graph."""
+        nat.lib()
+
+    def _router_for(self, graph: CompactHierarchicalGraph) -> GpuRouter:
+        key = id(graph)
+        hit = self._cache.get(key)
+        if hit is not None and hit[0]() is graph:
+            return hit[1]
+        index = DeviceIndex(graph, self.base_vecs, self.device)
+        router = GpuRouter(index, self.metric, self.topk, self.candidate_queue_size, mode=self.mode,
+                           schedule=self.schedule, **self.router_opts)
+        self._cache[key] = (weakref.ref(graph), router)
+        return router
+
+    def batch_query(self, query_vecs: np.ndarray, graph: CompactHierarchicalGraph) -> np.ndarray:
+        """knn_results_t: (nq * topk,) uint64 CandidateEntry words."""
+        out = self._router_for(graph).batch_query(query_vecs)
+        return out.reshape(-1)
+
+    def query(self, query_vec: np.ndarray, graph: CompactHierarchicalGraph) -> np.ndarray:
+        """query(): at most topk entries (the invalid tail is dropped)."""
+        words = self._router_for(graph).batch_query(np.asarray(query_vec, dtype=np.float32).reshape(1, -1))[0]
+        return words[~entry_is_invalid(words)]
+
+    def batch_query_l0_only(self, query_vecs: np.ndarray, graph: CompactHierarchicalGraph) -> np.ndarray:
+        out = self._router_for(graph).batch_query(query_vecs, l0_only=True)
+        return out.reshape(-1)
+
+    def close(self) -> None:
+        for _, (_, r) in list(self._cache.items()):
+            r.close()
+            r.index.close()
+        self._cache.clear()

@@ -1,0 +1,81 @@
+"""Workload preparation: seeded vectors plus a graph from the reference builder.
+
+The query path searches graphs built and compacted by the reference's own CPU
+builder (index_build/_ref/artea_build_index, the artea_graph factory +
+compactor + HGRA snapshot). Graphs are cached by the fingerprint of the exact
+vectors they index, so tests, smoke runs and benchmarks that share a workload
+build it once per machine. Concurrent processes (one per GPU) serialise on a
+lock file; the first builds, the others wait and reuse.
+"""
+
+from __future__ import annotations
+
+import fcntl
+import json
+import os
+import subprocess
+import time
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import datasets as ds
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BUILDER = os.path.join(ROOT, "index_build", "_ref", "artea_build_index")
+DEFAULT_CACHE = os.environ.get("ARTEA_CACHE", os.path.join(ROOT, ".cache"))
+
+BUILD_PARAMS = dict(beta=2.0, tau_k=0.0, tau=1.5, search_nn_qs=64, loops=15, triu=4, prefill=0.4, scale=1.10,
+                    shift=1.5, shuffle=1)
+
+
+def graph_for(base: np.ndarray, metric: str, l0: float = 1.0, cache_dir: Optional[str] = None,
+              tag: str = "graph", log=None) -> Tuple[str, dict]:
+    """Path of an HGRA snapshot for ``base`` (building it if needed) and the
+    builder's report (build seconds, level histogram, threads)."""
+    cache_dir = cache_dir or DEFAULT_CACHE
+    os.makedirs(cache_dir, exist_ok=True)
+    fp = ds.fingerprint(base)
+    stem = os.path.join(cache_dir, f"{tag}-{metric}-l0{l0:g}-{fp}")
+    hgra, meta = stem + ".hgra", stem + ".json"
+    lock = open(stem + ".lock", "w")
+    try:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        if os.path.exists(hgra) and os.path.exists(meta):
+            with open(meta) as f:
+                return hgra, json.load(f)
+        if not os.path.exists(BUILDER):
+            raise FileNotFoundError(f"{BUILDER} is missing: build it with `make -C index_build` where the "
+                                    "reference headers are available")
+        fbin = stem + ".fbin"
+        ds.write_fbin(fbin, base)
+        args = [BUILDER, "--base", fbin, "--metric", metric, "--out", hgra + ".tmp", "--l0", str(l0)]
+        for k, v in BUILD_PARAMS.items():
+            args += [f"--{k.replace('_', '-')}", str(v)]
+        t0 = time.time()
+        if log:
+            log(f"building {metric} graph over {base.shape[0]} x {base.shape[1]} with the reference builder ...")
+        res = subprocess.run(args, check=True, capture_output=True, text=True)
+        report = json.loads(res.stdout.strip().splitlines()[-1])
+        report["wall_s"] = time.time() - t0
+        os.replace(hgra + ".tmp", hgra)
+        os.remove(fbin)
+        with open(meta, "w") as f:
+            json.dump(report, f)
+        if log:
+            log(f"graph built in {report['wall_s']:.1f} s: levels {report['vertices_by_highest_level']}")
+        return hgra, report
+    finally:
+        fcntl.flock(lock, fcntl.LOCK_UN)
+        lock.close()
+
+
+def prepare(name: str, n_base: Optional[int] = None, n_query: Optional[int] = None, cache_dir: Optional[str] = None,
+            log=None):
+    """(workload, base, queries, hgra_path, build_report) for a named workload."""
+    w = ds.WORKLOADS[name]
+    if n_base is not None or n_query is not None:
+        w = w.scaled(n_base, n_query)
+    base, queries = ds.generate(w)
+    hgra, report = graph_for(base, w.metric, l0=w.l0_min_distance, cache_dir=cache_dir, tag=w.name, log=log)
+    return w, base, queries, hgra, report

@@ -1,0 +1,462 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 hierarchical-graph router (ARTEA batch_query).
+
+Metric: QPS at recall@100 >= 0.95. The default workload is the 1M x 128
+Euclidean SIFT-like index (seeded synthetic stand-in, 10,000 queries, topk
+100): the queue size is swept over {100, 200, 400, 800} and the smallest size
+whose recall@100 reaches 0.95 is timed. One step = one batch_query of all
+10,000 queries.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is device time (CUDA events around each launch on its stream, inputs
+already in HBM, L2 flushed between steps and excluded); `e2e` is the same
+metric through the public C-ABI with host buffers (H2D of queries and D2H of
+results inside the timed region). Multi-GPU runs are replicas (weak scaling):
+every rank holds the whole index and answers its own batch.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from artea_b200 import datasets as ds  # noqa: E402
+from artea_b200 import workload as wl  # noqa: E402
+
+METRIC_NAME = "QPS @ recall@100>=0.95"
+DEFAULT_QUEUES = (100, 200, 400, 800)
+
+
+def log(msg: str) -> None:
+    if int(os.environ.get("RANK", "0")) == 0:
+        print(f"[bench] {msg}", file=sys.stderr, flush=True)
+
+
+def host_has_avx512() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = f.read()
+        return all(f in flags for f in ("avx512f", "avx512bw", "avx512vl", "avx512dq", "avx512cd"))
+    except OSError:
+        return False
+
+
+def metric_code(name: str) -> int:
+    return {"euclidean": 0, "cosine": 2, "dot": 3}[name]
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region.
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines = []
+        self.window = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, t0: float, t1: float) -> None:
+        """Keep the samples taken between t0 and t1 (time.time())."""
+        self.window = (t0, t1)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        lines = self.lines
+        if self.window is not None:
+            inside = [l for l in lines if self.window[0] <= l[0] <= self.window[1] + 0.15]
+            lines = inside or lines
+        for _, line in lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 10:
+                continue
+            try:
+                sm.append(float(parts[2]))
+                mx = max(mx, float(parts[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[6:10]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Ground truth (exact top-k by distance, ties by vid), on the GPU with torch.
+# ---------------------------------------------------------------------------
+def ground_truth(base: np.ndarray, queries: np.ndarray, k: int, metric: str, device, cache_dir: str) -> np.ndarray:
+    import torch
+    path = os.path.join(cache_dir, f"gt-{metric}-{k}-{ds.fingerprint(base)}-{ds.fingerprint(queries)}.npy")
+    if os.path.exists(path):
+        return np.load(path)
+    torch.backends.cuda.matmul.allow_tf32 = False
+    xb = torch.from_numpy(base).to(device)
+    xb64 = xb.double()
+    xn = (xb * xb).sum(1)
+    out = np.empty((queries.shape[0], k), dtype=np.uint32)
+    extra = 64
+    for lo in range(0, queries.shape[0], 256):
+        q = torch.from_numpy(queries[lo:lo + 256]).to(device)
+        if metric == "euclidean":
+            d = (q * q).sum(1, keepdim=True) - 2.0 * (q @ xb.T) + xn[None, :]
+        elif metric == "cosine":
+            d = 1.0 - (q @ xb.T) / (q.norm(dim=1, keepdim=True) * xb.norm(dim=1)[None, :]).clamp_min(1e-30)
+        else:
+            d = -(q @ xb.T)
+        cand = torch.topk(d, min(k + extra, d.shape[1]), dim=1, largest=False).indices
+        q64 = q.double()[:, None, :]
+        rows = xb64[cand]
+        if metric == "euclidean":
+            ex = ((rows - q64) ** 2).sum(-1)
+        elif metric == "cosine":
+            ex = 1.0 - (rows * q64).sum(-1) / (rows.norm(dim=-1) * q64.norm(dim=-1)).clamp_min(1e-300)
+        else:
+            ex = -(rows * q64).sum(-1)
+        # sort by (distance, vid)
+        order = torch.argsort(cand, dim=1)
+        cand = torch.gather(cand, 1, order)
+        ex = torch.gather(ex, 1, order)
+        order = torch.argsort(ex, dim=1, stable=True)
+        out[lo:lo + 256] = torch.gather(cand, 1, order)[:, :k].cpu().numpy().astype(np.uint32)
+    del xb, xb64
+    np.save(path, out)
+    return out
+
+
+def recall(words: np.ndarray, gt: np.ndarray, k) -> float:
+    pred = (words & np.uint64(0x7FFFFFFF)).astype(np.int64)
+    ks = np.broadcast_to(np.asarray(k), (pred.shape[0],))
+    hits = 0
+    for i in range(pred.shape[0]):
+        kk = int(ks[i])
+        hits += len(set(pred[i, :kk].tolist()) & set(gt[i, :kk].tolist()))
+    return hits / float(ks.sum())
+
+
+def algorithmic_bytes(stats: np.ndarray, dim: int, k) -> np.ndarray:
+    """Bytes one query must move: its query row, one vector row per distance
+    evaluation, per row read the vertex record (8 B) and two CSR offsets
+    (16 B) plus 4 B per neighbour id, and its k result entries (8 B each)."""
+    st = stats.astype(np.float64)
+    rows = st[:, 1] + st[:, 3]
+    ids = st[:, 2] + st[:, 4]
+    return 4.0 * dim + st[:, 0] * 4.0 * dim + rows * 24.0 + ids * 4.0 + 8.0 * np.asarray(k, dtype=np.float64)
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profile_traffic(workload: str):
+    """dram read+write bytes per launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"search_kernel_{workload}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own batch_query on this host's cores.
+# ---------------------------------------------------------------------------
+def cpu_baseline(hgra: str, base: np.ndarray, queries: np.ndarray, topk: int, queue: int, metric: int,
+                 sample: int, repeats: int = 1) -> dict:
+    from oracle import oracle as orc
+    q = queries[:sample]
+    threads = os.cpu_count() or 1
+    if orc.have_ref() and host_has_avx512():
+        r = orc.RefRouter(hgra, base)
+        r.batch_query(q[: min(256, len(q))], topk, queue, metric=metric)   # warm-up
+        secs = []
+        for _ in range(repeats):
+            _, s = r.batch_query(q, topk, queue, metric=metric)
+            secs.append(s)
+        cores = int(orc.ref_lib().artea_ref_max_threads())
+        r.close()
+        kind = "reference"
+    else:
+        from artea_b200.graph import CompactHierarchicalGraph
+        g = CompactHierarchicalGraph.from_hgra(hgra)
+        orc.batch_query(g, base, q[: min(256, len(q))], topk, queue, metric=metric, threads=threads)
+        secs = []
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            orc.batch_query(g, base, q, topk, queue, metric=metric, threads=threads)
+            secs.append(time.perf_counter() - t0)
+        cores = threads
+        kind = "port"
+    s = statistics.mean(secs)
+    return {"value": len(q) / s, "unit": "queries/s", "cores": cores, "kind": kind,
+            "sample": f"{len(q)} queries x {repeats} run(s) of batch_query at queue {queue}, topk {topk}",
+            "seconds_per_run": s}
+
+
+# ---------------------------------------------------------------------------
+def run_reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w, base, queries, hgra, report = wl.prepare(args.workload, args.n_base, args.n_query, log=log)
+    queue = args.reference_queue or 200
+    sample = min(args.reference_sample, queries.shape[0])
+    vals = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        info = cpu_baseline(hgra, base, queries, w.topk, queue, metric_code(w.metric), sample)
+        if i >= args.warmup:
+            vals.append(info["value"])
+    value = statistics.mean(vals)
+    line = {"metric": METRIC_NAME, "value": value, "unit": "queries/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sample / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": w.name, "n_base": w.n_base, "n_query": sample,
+                                           "dim": w.dim, "metric": w.metric, "topk": w.topk, "queue": queue},
+            "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default="sift1m", choices=sorted(ds.WORKLOADS))
+    ap.add_argument("--n-base", type=int, default=None)
+    ap.add_argument("--n-query", type=int, default=None)
+    ap.add_argument("--mode", choices=("exact", "fast"), default="exact")
+    ap.add_argument("--schedule", choices=("auto", "plain", "persistent"), default="auto")
+    ap.add_argument("--queues", default=",".join(str(q) for q in DEFAULT_QUEUES))
+    ap.add_argument("--recall-target", type=float, default=0.95)
+    ap.add_argument("--cpu-sample", type=int, default=2000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-queue", type=int, default=0)
+    ap.add_argument("--reference-sample", type=int, default=2000)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import torch
+    from artea_b200.graph import CompactHierarchicalGraph
+    from artea_b200.router import DeviceIndex, GpuRouter
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+
+    w, base, queries, hgra, report = wl.prepare(args.workload, args.n_base, args.n_query, log=log)
+    metric = metric_code(w.metric)
+    nq, dim, k = queries.shape[0], base.shape[1], w.topk
+    graph = CompactHierarchicalGraph.from_hgra(hgra)
+    index = DeviceIndex(graph, base, device=local)
+    cache_dir = wl.DEFAULT_CACHE
+    gt = ground_truth(base, queries, k, w.metric, device, cache_dir) if rank == 0 else None
+
+    d_q = torch.from_numpy(queries).to(device)
+    d_out = torch.empty((nq, k), dtype=torch.int64, device=device)
+    d_stats = torch.zeros((nq, 8), dtype=torch.int32, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    def make_router(L):
+        return GpuRouter(index, metric, k, L, mode=args.mode, schedule=args.schedule, max_batch=nq)
+
+    # Queue sweep: recall per queue size (rank 0 decides, all ranks follow).
+    queues = [int(x) for x in args.queues.split(",") if x]
+    sweep = []
+    chosen = queues[-1]
+    for L in queues:
+        r = make_router(L)
+        r.batch_query_device(d_q, nq, k, d_out, stream=stream.cuda_stream)
+        torch.cuda.synchronize(device)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        r.batch_query_device(d_q, nq, k, d_out, stream=stream.cuda_stream)
+        t1.record(stream)
+        torch.cuda.synchronize(device)
+        ms = t0.elapsed_time(t1)
+        rec = recall(d_out.cpu().numpy().view(np.uint64), gt, k) if rank == 0 else 0.0
+        sweep.append({"queue": L, "recall": round(rec, 5), "qps": nq / (ms / 1e3)})
+        r.close()
+    if rank == 0:
+        ok = [s["queue"] for s in sweep if s["recall"] >= args.recall_target]
+        chosen = ok[0] if ok else queues[-1]
+    if dist is not None:
+        t = torch.tensor([chosen], device=device)
+        dist.broadcast(t, 0)
+        chosen = int(t.item())
+
+    router = make_router(chosen)
+    # Counters for the algorithmic-byte count (untimed).
+    router.batch_query_device(d_q, nq, k, d_out, d_stats=d_stats, stream=stream.cuda_stream)
+    torch.cuda.synchronize(device)
+    stats = d_stats.cpu().numpy().view(np.uint32)
+    words = d_out.cpu().numpy().view(np.uint64)
+    final_recall = recall(words, gt, k) if rank == 0 else 0.0
+    alg_bytes = float(algorithmic_bytes(stats, dim, k).sum())
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    for _ in range(args.warmup):
+        router.batch_query_device(d_q, nq, k, d_out, stream=stream.cuda_stream)
+    torch.cuda.synchronize(device)
+
+    launches0 = router.launches()
+    step_ms = []
+    with ClockSampler(local) as clocks:
+        time.sleep(0.5)   # let nvidia-smi start sampling
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+        t_start = time.time()
+        wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            router.batch_query_device(d_q, nq, k, d_out, stream=stream.cuda_stream)
+            e1.record(stream)
+            step_ms.append((e0, e1))
+        torch.cuda.synchronize(device)
+        if dist is not None:
+            dist.barrier()
+        wall = time.perf_counter() - wall0
+        clocks.mark(t_start, time.time())
+        time.sleep(0.2)
+    launches = router.launches() - launches0
+    router.sync()
+    ms = [a.elapsed_time(b) for a, b in step_ms]
+    mean_ms = statistics.mean(ms)
+    total_ms = sum(ms)
+    if dist is not None:
+        t = torch.tensor([total_ms, mean_ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, mean_ms = float(t[0]), float(t[1])
+    value = world * nq * args.steps / (total_ms / 1e3)
+
+    # End to end through the public API with host buffers.
+    hq = torch.from_numpy(queries).pin_memory().numpy()
+    e2e_s = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        out = router.batch_query(hq)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_s.append(dt)
+    e2e_launches = args.steps
+    e2e_mean = statistics.mean(e2e_s)
+    if dist is not None:
+        t = torch.tensor([e2e_mean], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_mean = float(t[0])
+    e2e_value = world * nq / e2e_mean
+    assert np.array_equal(out, words), "host-buffer API disagrees with the device-buffer API"
+
+    peaks = measured_peaks()
+    achieved = alg_bytes / (mean_ms / 1e3) / 1e9
+    traffic = profile_traffic(w.name)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peaks["source"],
+                "kernel": "search_persistent_kernel" if args.schedule != "plain" else "search_plain_kernel"}
+
+    baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        baseline = cpu_baseline(hgra, base, queries, k, chosen, metric, min(args.cpu_sample, nq))
+
+    if rank == 0:
+        st = stats.astype(np.float64)
+        line = {
+            "metric": METRIC_NAME, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w.name, "n_base": w.n_base, "n_query": nq, "dim": dim, "metric": w.metric,
+                       "topk": k, "queue": chosen, "mode": args.mode, "schedule": args.schedule,
+                       "recall_at_100": round(final_recall, 5), "parallelism": f"replicas{world}",
+                       "l2": "256 MiB buffer written between timed steps (excluded from timing); "
+                             "base vectors 512 MB > L2",
+                       "graph_levels": report.get("vertices_by_highest_level"),
+                       "graph_build_s": report.get("build_s")},
+            "sweep": sweep,
+            "e2e": {"value": e2e_value, "unit": "queries/s",
+                    "h2d_bytes_per_step": int(queries.nbytes), "d2h_bytes_per_step": int(nq * k * 8)},
+            "roofline": roofline,
+            "cpu_baseline": None if baseline is None else {kk: baseline[kk] for kk in
+                                                           ("value", "unit", "cores", "kind", "sample")},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "per_query": {"dist_evals": float(st[:, 0].mean()), "l0_rows": float(st[:, 3].mean()),
+                          "upper_rows": float(st[:, 1].mean()), "bytes": alg_bytes / nq},
+            "wall_s_timed_region": wall,
+        }
+        print(json.dumps(line), flush=True)
+    router.close()
+    index.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

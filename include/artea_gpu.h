@@ -1,0 +1,210 @@
+/*
+ * artea_gpu.h — C-ABI of the B200 query path for ARTEA compact hierarchical
+ * graphs. Plain pointers and sizes only; every function returns an
+ * artea_gpu_status and never throws. Thread safety: one index may be queried
+ * from several host threads only with distinct artea_gpu_router handles.
+ *
+ * What each entry point replaces in the reference (paths relative to the
+ * reference project root):
+ *
+ *   artea_gpu_index_create / _from_hgra  — the caller-owned inputs of
+ *       HierarchicalGraphRouter: base_vecs (router ctor,
+ *       include/artea/cpu/router/hierarchical_graph_router.hpp:93-109) and the
+ *       compact::HierarchicalGraph passed to batch_query
+ *       (include/artea/cpu/index/compact_structure/hierarchical_graph.hpp:33-201;
+ *       HGRA restore: include/artea/cpu/index/persistence/hierarchical_graph_file_manager.hpp:152).
+ *       Uploaded once; device resident afterwards.
+ *   artea_gpu_router_create — HierarchicalGraphRouter(base_vecs, dist_func, topk,
+ *       candidate_queue_size) + initialize() (hierarchical_graph_router.hpp:93-117):
+ *       fails with ARTEA_GPU_EINVAL when queue < topk, as the ctor throws.
+ *   artea_gpu_batch_query — batch_query<RandomSeeding=false, enable_early_stop=false>
+ *       (hierarchical_graph_router.hpp:293-349): host buffers in and out.
+ *   artea_gpu_batch_query_device — the same on device-resident buffers and a
+ *       caller stream (no host copies).
+ *   artea_gpu_batch_query_l0_only — batch_query_l0_only
+ *       (hierarchical_graph_router.hpp:353-385).
+ *   artea_gpu_hgra_probe / artea_gpu_hgra_read — HierarchicalGraphFileManager::restore
+ *       into caller buffers (hierarchical_graph_file_manager.hpp:15-39, 152-300).
+ *   artea_gpu_last_error — text of ARTEA_ERROR / exception messages
+ *       (include/artea/common/logger.hpp:97-99).
+ *
+ * Result words: each result is the 8-byte CandidateEntry
+ * (include/artea/cpu/router/data_structures/candidate_entry.hpp:57-65): low 32 bits
+ * vid | explored<<31, high 32 bits the float distance. Rows hold k_stride words;
+ * unused tail slots hold the invalid entry (vid 0x7FFFFFFF, FLT_MAX)
+ * (hierarchical_graph_router.hpp:334, candidate_entry.hpp:97-99).
+ */
+#ifndef ARTEA_GPU_H
+#define ARTEA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum artea_gpu_status {
+    ARTEA_GPU_OK = 0,
+    ARTEA_GPU_EINVAL = 1,    /* bad argument (sizes, queue < topk, metric, mode) */
+    ARTEA_GPU_ENOMEM = 2,    /* device or host allocation failed */
+    ARTEA_GPU_ECUDA = 3,     /* a CUDA runtime call failed */
+    ARTEA_GPU_EGRAPH = 4,    /* graph failed validation (ids out of range, bad rows) */
+    ARTEA_GPU_EIO = 5,       /* snapshot file missing, truncated or malformed */
+    ARTEA_GPU_EKERNEL = 6,   /* a kernel reported an internal error (bound exceeded) */
+    ARTEA_GPU_ETIMEOUT = 7,  /* a bounded wait gave up */
+    ARTEA_GPU_ENODEV = 8     /* no usable CUDA device */
+} artea_gpu_status;
+
+/* DistanceMetricsT values the router is instantiated with
+ * (include/artea/cpu/utils/simd_distance.hpp:64-79). Searches on Euclidean
+ * data use EUCLIDEAN_SQR, as search_infra_dispatch maps them
+ * (include/artea/cpu/framework/type_context/infra_dispatcher.hpp:234-241). */
+typedef enum artea_gpu_metric {
+    ARTEA_GPU_EUCLIDEAN_SQR = 0,
+    ARTEA_GPU_EUCLIDEAN = 1,
+    ARTEA_GPU_COSINE = 2,
+    ARTEA_GPU_DOT = 3
+} artea_gpu_metric;
+
+/* EXACT reproduces the reference's float summation order (16 lane partials
+ * + GCC reduction tree) and its queue's tie rules bit for bit. FAST sums in
+ * warp order and merges each neighbour batch into the queue in one step. */
+typedef enum artea_gpu_mode {
+    ARTEA_GPU_MODE_EXACT = 0,
+    ARTEA_GPU_MODE_FAST = 1
+} artea_gpu_mode;
+
+/* Kernel schedule. PLAIN: one CTA of one warp per query, grid = nq.
+ * PERSISTENT: a grid sized to the GPU whose warps take queries from a shared
+ * counter (work stealing); warps_per_cta chosen by the autotuner unless set. */
+typedef enum artea_gpu_schedule {
+    ARTEA_GPU_SCHEDULE_AUTO = 0,
+    ARTEA_GPU_SCHEDULE_PLAIN = 1,
+    ARTEA_GPU_SCHEDULE_PERSISTENT = 2
+} artea_gpu_schedule;
+
+/* compact::HierarchicalGraph in grouped-CSR form, host memory
+ * (include/artea/cpu/index/compact_structure/hierarchical_graph.hpp:46-49, 169-200).
+ * Group h lists the vertices whose highest level is h; it has
+ * group_sizes[h]*(h+1)+1 offsets, rows ordered level h down to 0 per vertex. */
+typedef struct artea_gpu_graph_desc {
+    uint32_t num_vertices;
+    uint32_t top_level;          /* 0xFFFFFFFF (or num_vertices == 0): empty graph */
+    uint32_t ul_max_nbr_size;
+    uint32_t bl_max_nbr_size;
+    uint32_t entry_point_vid;
+    const uint32_t* vertex_info; /* num_vertices x {highest_level, local_vid}; unassigned: {~0u, ~0u} */
+    const uint64_t* const* group_offsets; /* top_level+1 pointers */
+    const uint64_t* group_sizes; /* top_level+1 vertex counts */
+    const uint32_t* neighbor_ids;
+    uint64_t num_neighbor_ids;
+} artea_gpu_graph_desc;
+
+/* Header of an HGRA v1 snapshot plus the sizes needed to read it. */
+typedef struct artea_gpu_hgra_info {
+    uint32_t num_vertices;
+    uint32_t top_level;
+    uint32_t ul_max_nbr_size;
+    uint32_t bl_max_nbr_size;
+    uint32_t entry_point_vid;
+    uint32_t num_groups;         /* top_level + 1 */
+    uint64_t num_neighbor_ids;
+    uint64_t num_offsets;        /* sum over groups of group_sizes[h]*(h+1)+1 */
+    uint64_t group_sizes[64];    /* first num_groups used */
+} artea_gpu_hgra_info;
+
+/* Per-query work counters (optional output of a batch query). In EXACT mode
+ * they equal the reference's counts: distance calls, rows read per level. */
+typedef struct artea_gpu_query_stats {
+    uint32_t dist_evals;        /* distance evaluations, entry point included */
+    uint32_t upper_rows;        /* neighbour rows read on levels >= 1 (greedy hops) */
+    uint32_t upper_row_ids;     /* ids in those rows */
+    uint32_t l0_rows;           /* level-0 expansions */
+    uint32_t l0_row_ids;        /* ids in level-0 rows */
+    uint32_t upper_dist_evals;  /* distance evaluations on levels >= 1 */
+    uint32_t results;           /* valid result entries */
+    uint32_t visited_spills;    /* visited-list overflows (full bitset clear) */
+} artea_gpu_query_stats;
+
+typedef struct artea_gpu_index artea_gpu_index;
+typedef struct artea_gpu_router artea_gpu_router;
+
+/* Options of a router (artea_gpu_router_create). Zero-initialise, then set. */
+typedef struct artea_gpu_router_opts {
+    int metric;              /* artea_gpu_metric */
+    int mode;                /* artea_gpu_mode */
+    int schedule;            /* artea_gpu_schedule */
+    uint32_t warps_per_cta;  /* persistent schedule; 0 = autotuned */
+    uint32_t ctas_per_sm;    /* persistent schedule; 0 = as many as fit */
+    uint32_t max_batch;      /* largest nq one call may pass; 0 = 65536 */
+    uint32_t max_queue;      /* largest per-query queue size; 0 = candidate_queue_size */
+    uint32_t use_graphs;     /* capture launches in CUDA graphs and replay them */
+} artea_gpu_router_opts;
+
+/* Library / device information. */
+const char* artea_gpu_version(void);
+const char* artea_gpu_last_error(void);
+int artea_gpu_device_count(int* count);
+
+/* ---- HGRA v1 snapshots (host only; no GPU needed) ---- */
+int artea_gpu_hgra_probe(const char* path, artea_gpu_hgra_info* info);
+/* Fills caller buffers sized from the probe: vertex_info (2*num_vertices u32),
+ * offsets (num_offsets u64, groups concatenated in level order), neighbor_ids. */
+int artea_gpu_hgra_read(const char* path, uint32_t* vertex_info, uint64_t* offsets, uint32_t* neighbor_ids);
+/* Writes an HGRA v1 snapshot of a graph description. */
+int artea_gpu_hgra_write(const char* path, const artea_gpu_graph_desc* graph);
+/* Checks a graph description on the host (ids in range, rows within their
+ * level's capacity, every row id present on that level, monotone offsets). */
+int artea_gpu_graph_validate(const artea_gpu_graph_desc* graph);
+
+/* ---- Device-resident index ---- */
+/* Validates and uploads the graph and the num_vectors x dim FP32 rows (dim a
+ * multiple of 16, rows padded with zeros as the reference pads them). */
+int artea_gpu_index_create(const artea_gpu_graph_desc* graph, const float* vectors, uint32_t num_vectors,
+                           uint32_t dim, int device, artea_gpu_index** out);
+/* Same, reading the graph from an HGRA v1 snapshot. */
+int artea_gpu_index_create_from_hgra(const char* path, const float* vectors, uint32_t num_vectors,
+                                     uint32_t dim, int device, artea_gpu_index** out);
+int artea_gpu_index_destroy(artea_gpu_index* index);
+/* Device bytes held by the index (vectors + CSR). */
+int artea_gpu_index_bytes(const artea_gpu_index* index, uint64_t* bytes);
+
+/* ---- Router ---- */
+/* topk / candidate_queue_size are the defaults used when a call passes no
+ * per-query arrays. Fails with EINVAL if candidate_queue_size < topk. */
+int artea_gpu_router_create(artea_gpu_index* index, uint32_t topk, uint32_t candidate_queue_size,
+                            const artea_gpu_router_opts* opts, artea_gpu_router** out);
+int artea_gpu_router_destroy(artea_gpu_router* router);
+
+/* batch_query on host buffers: queries (nq x dim FP32, host) in, out_entries
+ * (nq x k_stride words, host) out; k_stride >= every topk. topk_per_query /
+ * queue_per_query may be NULL (router defaults). stats (nq, host) may be NULL.
+ * Includes the host<->device copies; synchronous. */
+int artea_gpu_batch_query(artea_gpu_router* router, const float* queries, uint32_t nq,
+                          const uint32_t* topk_per_query, const uint32_t* queue_per_query,
+                          uint32_t k_stride, uint64_t* out_entries, artea_gpu_query_stats* stats);
+
+/* Same on device buffers, enqueued on `stream` (a cudaStream_t; NULL = the
+ * CUDA default stream); returns without waiting. Buffers must be 16-byte
+ * aligned. Per-query arrays and stats are
+ * device pointers or NULL. */
+int artea_gpu_batch_query_device(artea_gpu_router* router, const float* d_queries, uint32_t nq,
+                                 const uint32_t* d_topk, const uint32_t* d_queue, uint32_t k_stride,
+                                 uint64_t* d_out, artea_gpu_query_stats* d_stats, void* stream);
+
+/* batch_query_l0_only on host buffers. */
+int artea_gpu_batch_query_l0_only(artea_gpu_router* router, const float* queries, uint32_t nq,
+                                  uint32_t k_stride, uint64_t* out_entries, artea_gpu_query_stats* stats);
+
+/* Waits for the router's stream and reports any kernel-side error. */
+int artea_gpu_router_sync(artea_gpu_router* router);
+
+/* Number of kernel launches this router has issued (for launch accounting). */
+int artea_gpu_router_launches(const artea_gpu_router* router, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ARTEA_GPU_H */

@@ -1,0 +1,74 @@
+"""Shared test helpers. GPU tests carry @pytest.mark.gpu; everything else runs on CPU."""
+import os
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+GOLDEN_CASES = ["early_stop_top0", "early_stop_top2", "early_stop_sqr", "axis80", "sift2k", "deep1k_cos", "gist400"]
+BUILDER = os.path.join(ROOT, "index_build", "_ref", "artea_build_index")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); run with -m gpu")
+
+
+class Case:
+    """One golden fixture: graph (from its HGRA bytes), vectors, queries and the
+    reference router's outputs per queue size."""
+
+    def __init__(self, name):
+        from artea_b200.graph import CompactHierarchicalGraph
+        z = np.load(os.path.join(GOLDEN, name + ".npz"))
+        self.name = name
+        self.base = z["base"].astype(np.float32)
+        self.queries = z["queries"]
+        self.metric = int(z["metric"])
+        self.topk = int(z["topk"])
+        self.queues = [int(x) for x in z["queues"]]
+        self.words = {L: z[f"words_L{L}"] for L in self.queues}
+        self.calls = {L: z[f"calls_L{L}"] for L in self.queues}
+        self.l0_words = {L: z[f"l0_words_L{L}"] for L in self.queues if f"l0_words_L{L}" in z}
+        self.l0_calls = {L: z[f"l0_calls_L{L}"] for L in self.queues if f"l0_calls_L{L}" in z}
+        fd, path = tempfile.mkstemp(suffix=".hgra")
+        with os.fdopen(fd, "wb") as f:
+            f.write(z["hgra"].tobytes())
+        self.hgra_path = path
+        self.graph = CompactHierarchicalGraph.from_hgra(path)
+
+
+_cases = {}
+
+
+def golden_case(name) -> Case:
+    if name not in _cases:
+        _cases[name] = Case(name)
+    return _cases[name]
+
+
+def build_graph(base, metric, workdir, **params):
+    """Runs the reference builder (prebuilt binary) on base; returns the HGRA path."""
+    import subprocess
+    from artea_b200 import datasets as ds
+    fbin = os.path.join(workdir, "base.fbin")
+    out = os.path.join(workdir, "graph.hgra")
+    ds.write_fbin(fbin, base)
+    args = [BUILDER, "--base", fbin, "--metric", metric, "--out", out]
+    for k, v in params.items():
+        args += [f"--{k.replace('_', '-')}", str(v)]
+    subprocess.run(args, check=True, stdout=subprocess.DEVNULL)
+    return out
+
+
+def gpu_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False

@@ -1,0 +1,156 @@
+"""Generates the golden fixtures of tests/golden from the ARTEA reference itself.
+
+Run in a container where the reference is mounted and built
+(``make -C oracle`` and ``make -C index_build``):
+
+    python tests/golden/make_golden.py
+
+Every expected output below comes from the reference's own code: graphs from
+its CPU builder (index_build/_ref/artea_build_index) and query results and
+distance-call counts from its hierarchical_graph_router_t (oracle/_ref). The
+hand-made graphs restate the shapes of the reference's unit tests
+(unit_tests/test_router_early_stop.cpp:59-97 and
+unit_tests/test_compact_csr_query.cpp:20-37); their expected answers are also
+re-derived independently (an exact sort) in the tests.
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from artea_b200 import datasets as ds  # noqa: E402
+from artea_b200.graph import CompactHierarchicalGraph, INVALID_LEVEL  # noqa: E402
+from oracle import oracle as orc  # noqa: E402
+
+BUILDER = os.path.join(ROOT, "index_build", "_ref", "artea_build_index")
+
+
+def early_stop_graph(top: int = 2) -> CompactHierarchicalGraph:
+    """4 vertices on one axis (x0 = 12, 8, 4, 0), dim 16; L2 singleton {0};
+    L1 chain 0->1->2->3; L0 complete (test_router_early_stop.cpp:69-97)."""
+    hl = [top if v == 0 else min(top, 1) for v in range(4)]
+    rows = []
+    for v in range(4):
+        r = {}
+        for h in range(hl[v] + 1):
+            if h == 0:
+                r[0] = [o for o in range(4) if o != v]
+            elif h == 1:
+                r[1] = [v + 1] if (top > 0 and v < 3) else []
+            else:
+                r[h] = []
+        rows.append(r)
+    return CompactHierarchicalGraph.from_rows(4, hl, rows, entry_point_vid=0, ul_max_nbr_size=4,
+                                              bl_max_nbr_size=4, top_level=top)
+
+
+def early_stop_vectors() -> np.ndarray:
+    v = np.zeros((4, 16), dtype=np.float32)
+    v[:, 0] = [12, 8, 4, 0]
+    return v
+
+
+def axis_graph() -> CompactHierarchicalGraph:
+    """80 vertices, dim 128, x0 = vid; vids < 40 on L1; complete rows (self
+    included) on every level, as the compactor leaves the rows of
+    test_compact_csr_query.cpp:24-37. Entry point: vid 19, the first vid
+    closest to the top bucket's centroid (x0 = 19.5)."""
+    hl = [1 if v < 40 else 0 for v in range(80)]
+    rows = [{0: list(range(80)), **({1: list(range(40))} if v < 40 else {})} for v in range(80)]
+    return CompactHierarchicalGraph.from_rows(80, hl, rows, entry_point_vid=19, ul_max_nbr_size=80,
+                                              bl_max_nbr_size=80, top_level=1)
+
+
+def axis_vectors() -> np.ndarray:
+    v = np.zeros((80, 128), dtype=np.float32)
+    v[:, 0] = np.arange(80, dtype=np.float32)
+    return v
+
+
+def axis_queries() -> np.ndarray:
+    q = np.zeros((5, 128), dtype=np.float32)
+    q[:, 0] = [-2.0, 12.25, 39.5, 60.75, 90.0]
+    return q
+
+
+def build_graph(base: np.ndarray, metric: str, workdir: str, **params) -> str:
+    fbin = os.path.join(workdir, "base.fbin")
+    out = os.path.join(workdir, "graph.hgra")
+    ds.write_fbin(fbin, base)
+    args = [BUILDER, "--base", fbin, "--metric", metric, "--out", out]
+    for k, v in params.items():
+        args += [f"--{k.replace('_', '-')}", str(v)]
+    subprocess.run(args, check=True, stdout=subprocess.DEVNULL)
+    return out
+
+
+def ref_results(hgra: str, base: np.ndarray, queries: np.ndarray, topk: int, queue: int, metric: int,
+                l0_only: bool = False):
+    r = orc.RefRouter(hgra, base)
+    words, _ = r.batch_query(queries, topk, queue, metric=metric, l0_only=l0_only, threads=4)
+    _, _, calls = r.batch_query(queries, topk, queue, metric=metric, l0_only=l0_only, count_distances=True)
+    r.close()
+    return words, calls
+
+
+def save_case(name: str, graph: CompactHierarchicalGraph, base: np.ndarray, queries: np.ndarray, metric: int,
+              topk: int, queues, base_dtype=np.float32, l0_only=False) -> None:
+    with tempfile.TemporaryDirectory() as tmp:
+        hgra = os.path.join(tmp, "g.hgra")
+        graph.to_hgra(hgra)
+        payload = {
+            "hgra": np.frombuffer(open(hgra, "rb").read(), dtype=np.uint8),
+            "base": base.astype(base_dtype),
+            "queries": queries.astype(np.float32),
+            "metric": np.int32(metric),
+            "topk": np.int32(topk),
+            "queues": np.asarray(queues, dtype=np.int32),
+        }
+        for L in queues:
+            words, calls = ref_results(hgra, base, queries, topk, L, metric)
+            payload[f"words_L{L}"] = words
+            payload[f"calls_L{L}"] = calls
+            if l0_only:
+                w0, c0 = ref_results(hgra, base, queries, topk, L, metric, l0_only=True)
+                payload[f"l0_words_L{L}"] = w0
+                payload[f"l0_calls_L{L}"] = c0
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **payload)
+    print(name, {k: v.shape for k, v in payload.items()})
+
+
+def built_case(name: str, workload: str, n_base: int, n_query: int, metric_build: str, metric: int, topk: int,
+               queues, quantize_u8: bool = False, **params) -> None:
+    w = ds.WORKLOADS[workload].scaled(n_base, n_query)
+    base, queries = ds.generate(w)
+    with tempfile.TemporaryDirectory() as tmp:
+        hgra = build_graph(base, metric_build, tmp, **params)
+        graph = CompactHierarchicalGraph.from_hgra(hgra)
+    save_case(name, graph, base, queries, metric, topk, queues,
+              base_dtype=np.uint8 if quantize_u8 else np.float32, l0_only=True)
+
+
+def main() -> None:
+    # Hand-made graphs from the reference unit tests.
+    for top in (0, 2):
+        save_case(f"early_stop_top{top}", early_stop_graph(top), early_stop_vectors(), early_stop_vectors(),
+                  metric=1, topk=1, queues=[4])
+    save_case("early_stop_sqr", early_stop_graph(2), early_stop_vectors(), early_stop_vectors(), metric=0, topk=1,
+              queues=[4])
+    save_case("axis80", axis_graph(), axis_vectors(), axis_queries(), metric=0, topk=10, queues=[80, 10, 16])
+    # Graphs from the reference builder on seeded synthetic data.
+    built_case("sift2k", "sift100k", 2000, 64, "euclidean", 0, 10, [10, 32, 100], quantize_u8=True)
+    built_case("deep1k_cos", "deep10m", 1000, 48, "cosine", 2, 10, [16, 64])
+    built_case("gist400", "gist1m", 400, 24, "euclidean", 0, 10, [20, 50], l0=0.05)
+
+
+if __name__ == "__main__":
+    main()

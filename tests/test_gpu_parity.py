@@ -1,0 +1,193 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the reference's own
+outputs (golden fixtures) and the oracle on seeded inputs. EXACT mode must be
+bit-identical (ids, float distances, distance-call counts); FAST mode must
+agree on >= 99.9% of top-k ids with distances within 1e-6 relative."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import BUILDER, GOLDEN_CASES, build_graph, golden_case
+from artea_b200 import datasets as ds
+from artea_b200.graph import CompactHierarchicalGraph
+from artea_b200.router import DeviceIndex, GpuRouter, HierarchicalGraphRouter, entry_dists, entry_vids
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+FAST_ID_AGREEMENT = 0.999
+# FAST distances agree with EXACT to 1e-6 relative. Cosine distance is
+# 1 - dot/|q||x|: near 0 any change of summation order is amplified by the
+# cancellation, so for cosine the 1e-6 is taken relative to max(|d|, 1), i.e.
+# 1e-6 absolute on its [0, 2] range.
+FAST_DIST_RTOL = 1e-6
+
+
+def fast_dist_ok(d_fast, d_exact, metric):
+    scale = max(abs(d_exact), 1.0) if metric == 2 else abs(d_exact)
+    return abs(d_fast - d_exact) <= FAST_DIST_RTOL * scale + 1e-30
+
+_indexes = {}
+
+
+def index_for(name):
+    if name not in _indexes:
+        c = golden_case(name)
+        _indexes[name] = DeviceIndex(c.graph, c.base)
+    return _indexes[name]
+
+
+@pytest.mark.parametrize("schedule", ["plain", "persistent"])
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_exact_matches_reference_bit_for_bit(name, schedule):
+    c = golden_case(name)
+    idx = index_for(name)
+    for L in c.queues:
+        r = GpuRouter(idx, c.metric, c.topk, L, mode="exact", schedule=schedule)
+        out, st = r.batch_query(c.queries, stats=True)
+        np.testing.assert_array_equal(out, c.words[L], err_msg=f"{name} L={L} {schedule}")
+        np.testing.assert_array_equal(st[:, 0].astype(np.uint64), c.calls[L], err_msg=f"{name} L={L} calls")
+        r.close()
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_exact_counters_match_oracle(name):
+    c = golden_case(name)
+    idx = index_for(name)
+    L = c.queues[-1]
+    r = GpuRouter(idx, c.metric, c.topk, L, mode="exact", schedule="persistent")
+    _, st = r.batch_query(c.queries, stats=True)
+    _, ost = orc.batch_query(c.graph, c.base, c.queries, c.topk, L, metric=c.metric, stats=True)
+    np.testing.assert_array_equal(st[:, :7], ost[:, :7])
+
+
+@pytest.mark.parametrize("name", ["sift2k", "deep1k_cos", "gist400"])
+def test_l0_only_matches_reference(name):
+    c = golden_case(name)
+    idx = index_for(name)
+    for L in c.queues:
+        r = GpuRouter(idx, c.metric, c.topk, L, mode="exact")
+        out, st = r.batch_query(c.queries, stats=True, l0_only=True)
+        np.testing.assert_array_equal(out, c.l0_words[L])
+        np.testing.assert_array_equal(st[:, 0].astype(np.uint64), c.l0_calls[L])
+
+
+def test_drop_in_router_surface_matches_reference():
+    c = golden_case("sift2k")
+    router = HierarchicalGraphRouter(c.base, "euclidean_sqr", topk=10, candidate_queue_size=32)
+    router.initialize()
+    words = router.batch_query(c.queries, c.graph)
+    assert words.shape == (c.queries.shape[0] * 10,)
+    np.testing.assert_array_equal(words.reshape(-1, 10), c.words[32])
+    one = router.query(c.queries[5], c.graph)
+    np.testing.assert_array_equal(one, c.words[32][5])
+    router.close()
+
+
+def _fast_agreement(exact, fast):
+    ev, fv = entry_vids(exact), entry_vids(fast)
+    agree = sum(len(set(a) & set(b)) for a, b in zip(ev, fv))
+    return agree / ev.size
+
+
+@pytest.mark.parametrize("name", ["sift2k", "deep1k_cos", "gist400"])
+def test_fast_mode_within_tolerance(name):
+    c = golden_case(name)
+    idx = index_for(name)
+    L = c.queues[-1]
+    ex = GpuRouter(idx, c.metric, c.topk, L, mode="exact").batch_query(c.queries)
+    fa = GpuRouter(idx, c.metric, c.topk, L, mode="fast").batch_query(c.queries)
+    assert _fast_agreement(ex, fa) >= FAST_ID_AGREEMENT - 0.02   # tiny fixtures: a single swap is 1/240
+    # distances of ids found by both modes agree to 1e-6 relative
+    for a, b in zip(ex, fa):
+        da = dict(zip(entry_vids(a).tolist(), entry_dists(a).tolist()))
+        for v, d in zip(entry_vids(b).tolist(), entry_dists(b).tolist()):
+            if v in da:
+                assert fast_dist_ok(d, da[v], c.metric), (v, d, da[v])
+
+
+@pytest.fixture(scope="module")
+def sift20k():
+    if not os.path.exists(BUILDER):
+        pytest.skip("index builder not built")
+    w = ds.WORKLOADS["sift100k"].scaled(20000, 512)
+    base, queries = ds.generate(w)
+    with tempfile.TemporaryDirectory() as tmp:
+        g = CompactHierarchicalGraph.from_hgra(build_graph(base, "euclidean", tmp))
+    return g, base, queries
+
+
+def test_uneven_per_query_topk_and_queue_exact(sift20k):
+    g, base, queries = sift20k
+    nq = queries.shape[0]
+    rng = np.random.default_rng(11)
+    topk = rng.choice(np.array([10, 100], np.uint32), nq)
+    queue = np.maximum(rng.choice(np.array([64, 128, 256, 512], np.uint32), nq), topk)
+    idx = DeviceIndex(g, base)
+    r = GpuRouter(idx, 0, 100, 512, mode="exact", schedule="persistent")
+    out, st = r.batch_query(queries, topk=topk, queue=queue, k_stride=100, stats=True)
+    ref, ost = orc.batch_query(g, base, queries, topk, queue, metric=0, k_stride=100, stats=True)
+    np.testing.assert_array_equal(out, ref)
+    np.testing.assert_array_equal(st[:, :7], ost[:, :7])
+
+
+@pytest.mark.parametrize("L", [100, 200, 400, 800])
+def test_exact_queue_sweep_against_oracle(sift20k, L):
+    g, base, queries = sift20k
+    idx = DeviceIndex(g, base)
+    for schedule in ("plain", "persistent"):
+        r = GpuRouter(idx, 0, 100, L, mode="exact", schedule=schedule)
+        out = r.batch_query(queries[:256])
+        ref = orc.batch_query(g, base, queries[:256], 100, L, metric=0)
+        np.testing.assert_array_equal(out, ref, err_msg=f"L={L} {schedule}")
+
+
+def test_fast_mode_agreement_and_recall(sift20k):
+    g, base, queries = sift20k
+    idx = DeviceIndex(g, base)
+    ex = GpuRouter(idx, 0, 100, 200, mode="exact").batch_query(queries)
+    fa = GpuRouter(idx, 0, 100, 200, mode="fast").batch_query(queries)
+    assert _fast_agreement(ex, fa) >= FAST_ID_AGREEMENT
+    gt, _ = orc.bruteforce(base, queries, 100)
+    assert abs(orc.recall_at_k(ex, gt, 100) - orc.recall_at_k(fa, gt, 100)) <= 0.002
+
+
+def test_batch_equals_single_queries():
+    c = golden_case("deep1k_cos")
+    idx = index_for("deep1k_cos")
+    r = GpuRouter(idx, c.metric, c.topk, 64)
+    batch = r.batch_query(c.queries)
+    for i in range(0, c.queries.shape[0], 7):
+        np.testing.assert_array_equal(r.batch_query(c.queries[i:i + 1])[0], batch[i])
+
+
+def test_repeated_calls_reuse_visited_state_cleanly():
+    c = golden_case("sift2k")
+    idx = index_for("sift2k")
+    r = GpuRouter(idx, c.metric, c.topk, 100, schedule="persistent")
+    first = r.batch_query(c.queries)
+    for _ in range(3):
+        np.testing.assert_array_equal(r.batch_query(c.queries), first)
+    np.testing.assert_array_equal(first, c.words[100])
+
+
+def test_empty_graph_returns_invalid_rows():
+    g = CompactHierarchicalGraph(0, 0, 4, 4, 0xFFFFFFFF, np.zeros((0, 2), np.uint32), [np.zeros(1, np.uint64)],
+                                 np.zeros(0, np.uint32))
+    base = np.zeros((4, 16), np.float32)
+    idx = DeviceIndex(g, base)
+    r = GpuRouter(idx, 1, 1, 4)
+    out = r.batch_query(np.zeros((3, 16), np.float32))
+    assert (entry_vids(out) == 0x7FFFFFFF).all()
+    assert (entry_dists(out) == np.finfo(np.float32).max).all()
+
+
+def test_topk_larger_than_found_keeps_invalid_tail():
+    c = golden_case("early_stop_top0")
+    idx = index_for("early_stop_top0")
+    r = GpuRouter(idx, 1, 4, 8)
+    out = r.batch_query(c.queries, k_stride=6)
+    ref = orc.batch_query(c.graph, c.base, c.queries, 4, 8, metric=1, k_stride=6)
+    np.testing.assert_array_equal(out, ref)
+    assert (entry_vids(out[:, 4:]) == 0x7FFFFFFF).all()

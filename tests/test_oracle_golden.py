@@ -1,0 +1,118 @@
+"""The oracle (C restatement) against the reference's own outputs and known answers."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, golden_case
+from oracle import oracle as orc
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_matches_reference_words_and_calls(name):
+    c = golden_case(name)
+    for L in c.queues:
+        out, st = orc.batch_query(c.graph, c.base, c.queries, c.topk, L, metric=c.metric, stats=True, threads=4)
+        np.testing.assert_array_equal(out, c.words[L], err_msg=f"{name} L={L}")
+        np.testing.assert_array_equal(st[:, 0].astype(np.uint64), c.calls[L], err_msg=f"{name} L={L} calls")
+
+
+@pytest.mark.parametrize("name", [n for n in GOLDEN_CASES if n in ("sift2k", "deep1k_cos", "gist400")])
+def test_oracle_l0_only_matches_reference(name):
+    c = golden_case(name)
+    for L in c.queues:
+        out, st = orc.batch_query(c.graph, c.base, c.queries, c.topk, L, metric=c.metric, l0_only=True,
+                                  stats=True, threads=4)
+        np.testing.assert_array_equal(out, c.l0_words[L])
+        np.testing.assert_array_equal(st[:, 0].astype(np.uint64), c.l0_calls[L])
+
+
+def test_early_stop_graph_default_query_makes_seven_distance_calls():
+    # unit_tests/test_router_early_stop.cpp:121-129: query = vector 3, topk 1,
+    # queue 4 -> result vid 3 after exactly 7 distance calls.
+    c = golden_case("early_stop_top2")
+    out, st = orc.batch_query(c.graph, c.base, c.queries[3:4], 1, 4, metric=1, stats=True)
+    assert (int(out[0, 0]) & 0x7FFFFFFF) == 3
+    assert st[0, 0] == 7
+
+
+def test_early_stop_batch_equals_per_query():
+    # test_router_early_stop.cpp:155-157: batch row i returns vid i.
+    c = golden_case("early_stop_top2")
+    out = orc.batch_query(c.graph, c.base, c.queries, 1, 4, metric=1)
+    assert [int(w) & 0x7FFFFFFF for w in out[:, 0]] == [0, 1, 2, 3]
+
+
+def test_axis80_top10_is_exact_sort_with_ties():
+    # test_compact_csr_query.cpp:48-74: results equal an exact sort by
+    # (distance, vid), tied distances included.
+    c = golden_case("axis80")
+    for L in c.queues:
+        out = orc.batch_query(c.graph, c.base, c.queries, 10, L, metric=0)
+        for i, q in enumerate(c.queries):
+            d = np.array([orc.distance(0, q, x) for x in c.base], dtype=np.float32)
+            order = sorted(range(80), key=lambda v: (d[v], v))[:10]
+            got = [int(w) & 0x7FFFFFFF for w in out[i]]
+            if L >= 80:
+                assert got == order
+            gd = (out[i] >> np.uint64(32)).astype(np.uint32).view(np.float32)
+            np.testing.assert_array_equal(gd, d[got])
+
+
+@pytest.mark.parametrize("dim", [16, 48, 96, 112, 128, 304, 384, 960])
+def test_euclidean_known_answer(dim):
+    # test_euclidean_distance.cpp:84-98: b = (3, 0, ..., 0, 4) -> 5.
+    a = np.zeros(dim, np.float32)
+    b = np.zeros(dim, np.float32)
+    b[0], b[-1] = 3.0, 4.0
+    assert orc.distance(1, a, b) == 5.0
+    assert orc.distance(0, a, b) == 25.0
+    assert orc.distance(0, a, a) == 0.0
+
+
+def test_cosine_edge_cases():
+    # test_cosine_distance.cpp:90-111.
+    rng = np.random.default_rng(7)
+    a = rng.standard_normal(96).astype(np.float32)
+    assert abs(orc.distance(2, a, a)) < 1e-5
+    assert abs(orc.distance(2, a, (a * np.float32(3.5)).astype(np.float32))) < 1e-5
+    assert abs(orc.distance(2, a, -a) - 2.0) < 1e-5
+    z = np.zeros(96, np.float32)
+    assert orc.distance(2, z, a) == 1.0
+    assert orc.distance(2, z, z) == 1.0
+
+
+def test_dot_is_negated_inner_product():
+    rng = np.random.default_rng(8)
+    a = rng.standard_normal(128).astype(np.float32)
+    b = rng.standard_normal(128).astype(np.float32)
+    assert abs(orc.distance(3, a, b) + float(np.dot(a.astype(np.float64), b))) < 1e-4
+
+
+@pytest.mark.parametrize("metric", [0, 1, 2, 3])
+@pytest.mark.parametrize("dim", [16, 96, 128, 960])
+def test_distance_bit_exact_against_reference_kernel(metric, dim):
+    if not orc.have_ref():
+        pytest.skip("reference router not built here")
+    rng = np.random.default_rng(metric * 1000 + dim)
+    for _ in range(50):
+        a = (rng.standard_normal(dim) * rng.uniform(0.01, 100)).astype(np.float32)
+        b = (rng.standard_normal(dim) * rng.uniform(0.01, 100)).astype(np.float32)
+        x = np.float32(orc.distance(metric, a, b))
+        y = np.float32(orc.ref_distance(metric, a, b))
+        assert x.view(np.uint32) == y.view(np.uint32)
+
+
+def test_scalar_double_reference_within_tolerance():
+    # test_euclidean_distance.cpp:67-82: within 2e-6 relative of a double sum.
+    rng = np.random.default_rng(3)
+    for dim in (16, 96, 128, 960):
+        a = rng.standard_normal(dim).astype(np.float32)
+        b = rng.standard_normal(dim).astype(np.float32)
+        ref = float(np.sum((a.astype(np.float64) - b) ** 2))
+        assert abs(orc.distance(0, a, b) - ref) <= 2e-6 * ref
+
+
+def test_recall_estimator_semantics():
+    # recall_estimator.hpp:150-230: duplicates in predictions count once.
+    words = np.array([[1, 1, 2], [5, 6, 7]], dtype=np.uint64)
+    gt = np.array([[1, 2, 3], [7, 8, 9]], dtype=np.uint32)
+    assert orc.recall_at_k(words, gt, 3) == pytest.approx(3 / 6)
