@@ -76,6 +76,8 @@ class RouterOpts(ctypes.Structure):
         ("max_batch", c_uint32),
         ("max_queue", c_uint32),
         ("use_graphs", c_uint32),
+        ("visited_hash_bits", c_uint32),
+        ("register_budget", c_uint32),
     ]
 
 
@@ -102,6 +104,8 @@ SIGNATURES = {
     "artea_gpu_batch_query_l0_only": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_void_p, c_void_p]),
     "artea_gpu_router_sync": (c_int, [c_void_p]),
     "artea_gpu_router_launches": (c_int, [c_void_p, POINTER(c_uint64)]),
+    "artea_gpu_router_set_phase_buffer": (c_int, [c_void_p, c_void_p]),
+    "artea_gpu_router_tuning": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32)]),
 }
 
 

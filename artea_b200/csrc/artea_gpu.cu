@@ -44,6 +44,7 @@ struct artea_gpu_index {
     uint2* d_vinfo = nullptr;
     uint32_t* d_nbrs = nullptr;
     uint64_t* d_offsets = nullptr;
+    unsigned long long* d_l0row = nullptr;
     const uint64_t* group_ptr[artea_gpu::kMaxGroups] = {};
     uint64_t bytes = 0;
 };
@@ -54,11 +55,19 @@ struct LaunchShape {
     uint32_t slots = 0;       // visited slots needed
 };
 
+// One point of the tuning space: warps per CTA, log2 of the shared-memory
+// visited hash size (0: no hash, the HBM bitset only) and register budget.
+struct Tuning {
+    uint32_t warps = 4;
+    uint32_t vh_bits = 11;
+    uint32_t regs = 0;   // 0: 85-register budget, 1: 64-register budget
+};
+
 struct artea_gpu_router {
     artea_gpu_index* idx = nullptr;
     uint32_t topk = 0, queue = 0, max_queue = 0, cap = 0, max_batch = 0;
     int metric = 0, mode = 0, schedule = 0;
-    uint32_t want_warps = 0, want_ctas_per_sm = 0;
+    uint32_t want_warps = 0, want_ctas_per_sm = 0, want_vh_bits = 0, want_regs = 0;
     bool use_graphs = false;
     cudaStream_t stream = nullptr;
     int num_sms = 0;
@@ -82,13 +91,19 @@ struct artea_gpu_router {
     uint32_t stage_nq = 0, stage_kstride = 0;
 
     uint64_t launches = 0;
-    std::map<uint64_t, uint32_t> tuned_warps;   // (dim, max queue) -> warps per CTA
-    std::map<uint32_t, LaunchShape> shapes;     // warps per CTA -> persistent grid
+    unsigned long long* d_phase = nullptr;      // optional per-query phase cycles (caller-owned)
+    std::map<uint64_t, Tuning> tuned;           // (dim, queue capacity) -> launch parameters
+    std::map<uint64_t, LaunchShape> shapes;     // (warps, hash bits) -> persistent grid
+    Tuning last;                                // parameters of the last launch
 };
 
 namespace {
 
 using namespace artea_gpu;
+
+// Router option visited_hash_bits: 0 = autotuned, ~0u = no hash, else log2 size.
+constexpr uint32_t kNoHash = 0xffffffffu;
+uint32_t hash_bits_of(uint32_t want) { return want == kNoHash ? 0u : want; }
 
 struct DeviceGuard {
     int prev = -1;
@@ -123,23 +138,30 @@ void dev_free(T*& p) {
 
 using KernelFn = void (*)(SearchArgs);
 
+// regs: 0 = 85-register budget, 1 = 64-register budget (persistent only).
 template <int kMetric>
-KernelFn pick_kernel_m(bool exact, bool persistent) {
-    if (persistent) return exact ? search_persistent_kernel<kMetric, true> : search_persistent_kernel<kMetric, false>;
+KernelFn pick_kernel_m(bool exact, bool persistent, uint32_t regs) {
+    if (persistent) {
+        if (regs == 1)
+            return exact ? search_persistent_kernel<kMetric, true, 4> : search_persistent_kernel<kMetric, false, 4>;
+        return exact ? search_persistent_kernel<kMetric, true, 3> : search_persistent_kernel<kMetric, false, 3>;
+    }
     return exact ? search_plain_kernel<kMetric, true> : search_plain_kernel<kMetric, false>;
 }
 
-KernelFn pick_kernel(int metric, bool exact, bool persistent) {
+KernelFn pick_kernel(int metric, bool exact, bool persistent, uint32_t regs = 0) {
     switch (metric) {
-        case ARTEA_GPU_EUCLIDEAN_SQR: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN_SQR>(exact, persistent);
-        case ARTEA_GPU_EUCLIDEAN: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN>(exact, persistent);
-        case ARTEA_GPU_COSINE: return pick_kernel_m<ARTEA_GPU_COSINE>(exact, persistent);
-        case ARTEA_GPU_DOT: return pick_kernel_m<ARTEA_GPU_DOT>(exact, persistent);
+        case ARTEA_GPU_EUCLIDEAN_SQR: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN_SQR>(exact, persistent, regs);
+        case ARTEA_GPU_EUCLIDEAN: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN>(exact, persistent, regs);
+        case ARTEA_GPU_COSINE: return pick_kernel_m<ARTEA_GPU_COSINE>(exact, persistent, regs);
+        case ARTEA_GPU_DOT: return pick_kernel_m<ARTEA_GPU_DOT>(exact, persistent, regs);
         default: return nullptr;
     }
 }
 
-uint32_t smem_bytes_per_warp(uint32_t dim, uint32_t cap) { return warp_smem_words(dim, cap) * 4u; }
+uint32_t smem_bytes_per_warp(uint32_t dim, uint32_t cap, uint32_t vh_bits) {
+    return warp_smem_words(dim, cap, vh_bits) * 4u;
+}
 
 int ensure_slots(artea_gpu_router* r, uint32_t slots) {
     if (slots <= r->slots) return ARTEA_GPU_OK;
@@ -174,26 +196,28 @@ int ensure_stage(artea_gpu_router* r, uint32_t nq, uint32_t k_stride) {
     return ARTEA_GPU_OK;
 }
 
-// Persistent grid for a warp count: as many CTAs per SM as fit.
-int persistent_shape(artea_gpu_router* r, uint32_t warps, LaunchShape* s) {
-    auto hit = r->shapes.find(warps);
+// Persistent grid for a tuning point: as many CTAs per SM as fit.
+int persistent_shape(artea_gpu_router* r, const Tuning& t, LaunchShape* s) {
+    const uint64_t key = (static_cast<uint64_t>(t.warps) << 32) | (t.vh_bits << 1) | t.regs;
+    auto hit = r->shapes.find(key);
     if (hit != r->shapes.end()) {
         *s = hit->second;
         return ARTEA_GPU_OK;
     }
-    KernelFn fn = pick_kernel(r->metric, r->mode == ARTEA_GPU_MODE_EXACT, true);
-    const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap) * warps;
+    KernelFn fn = pick_kernel(r->metric, r->mode == ARTEA_GPU_MODE_EXACT, true, t.regs);
+    const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) * t.warps;
+    if (smem > 227u * 1024u) return fail(ARTEA_GPU_EINVAL, "persistent CTA needs more than 227 KB shared memory");
     CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(fn),
-                                                           static_cast<int>(warps * 32), smem));
+                                                           static_cast<int>(t.warps * 32), smem));
     if (per_sm <= 0) return fail(ARTEA_GPU_EINVAL, "persistent kernel does not fit on an SM (queue too large?)");
     if (r->want_ctas_per_sm) per_sm = std::min<int>(per_sm, static_cast<int>(r->want_ctas_per_sm));
-    s->warps_per_cta = warps;
+    s->warps_per_cta = t.warps;
     s->ctas = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(r->num_sms);
-    s->slots = s->ctas * warps;
-    r->shapes[warps] = *s;
+    s->slots = s->ctas * t.warps;
+    r->shapes[key] = *s;
     return ARTEA_GPU_OK;
 }
 
@@ -205,6 +229,7 @@ int fill_args(artea_gpu_router* r, SearchArgs* a, const float* d_q, uint32_t nq,
     a->g.vecs = ix->d_vecs;
     a->g.vinfo = ix->d_vinfo;
     a->g.nbrs = ix->d_nbrs;
+    a->g.l0row = ix->d_l0row;
     a->g.n = ix->n;
     a->g.dim = ix->dim;
     a->g.top = ix->top;
@@ -227,78 +252,111 @@ int fill_args(artea_gpu_router* r, SearchArgs* a, const float* d_q, uint32_t nq,
     a->next_query = r->d_counter;
     a->error = r->d_error;
     a->l0_only = l0_only ? 1u : 0u;
+    a->phase_cycles = r->d_phase;
     return ARTEA_GPU_OK;
 }
 
-int launch_with(artea_gpu_router* r, SearchArgs a, bool persistent, uint32_t warps, cudaStream_t st) {
+int launch_with(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning& t, cudaStream_t st) {
     const bool exact = r->mode == ARTEA_GPU_MODE_EXACT;
-    KernelFn fn = pick_kernel(r->metric, exact, persistent);
+    KernelFn fn = pick_kernel(r->metric, exact, persistent, t.regs);
     if (!fn) return fail(ARTEA_GPU_EINVAL, "unknown metric");
     if (a.nq == 0) return ARTEA_GPU_OK;
+    a.vh_bits = t.vh_bits;
+    {
+        uint32_t kb = 1;
+        while (kb < 32 && (1ull << kb) < r->idx->n) ++kb;
+        if (a.vh_bits && kb < a.vh_bits + 1) kb = a.vh_bits + 1;
+        a.vk_bits = kb;
+        // The 16-bit quotient (with 0xFFFF reserved) must hold kbits - tbits bits.
+        if (a.vh_bits && kb - a.vh_bits >= 16) return fail(ARTEA_GPU_EINVAL, "visited table too small for N");
+    }
     if (persistent) {
         LaunchShape s;
-        if (int rc = persistent_shape(r, warps, &s)) return rc;
-        const uint32_t needed_ctas = (a.nq + warps - 1) / warps;
+        if (int rc = persistent_shape(r, t, &s)) return rc;
+        const uint32_t needed_ctas = (a.nq + t.warps - 1) / t.warps;
         const uint32_t ctas = std::min(s.ctas, needed_ctas);
-        if (int rc = ensure_slots(r, ctas * warps)) return rc;
+        if (int rc = ensure_slots(r, ctas * t.warps)) return rc;
         a.vis_bits = r->d_vis_bits;
         a.vis_list = r->d_vis_list;
         CUDA_TRY(cudaMemsetAsync(r->d_counter, 0, sizeof(uint32_t), st));
-        const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap) * warps;
-        fn<<<ctas, warps * 32, smem, st>>>(a);
+        const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) * t.warps;
+        fn<<<ctas, t.warps * 32, smem, st>>>(a);
     } else {
         if (int rc = ensure_slots(r, a.nq)) return rc;
         a.vis_bits = r->d_vis_bits;
         a.vis_list = r->d_vis_list;
-        const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap);
+        const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits);
         CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         fn<<<a.nq, 32, smem, st>>>(a);
     }
+    r->last = t;
     r->launches++;
     CUDA_TRY(cudaGetLastError());
     return ARTEA_GPU_OK;
 }
 
-// Autotuner: warps per CTA for the persistent schedule, picked per
-// (dim, queue capacity) by timing each candidate on the first call's batch.
-int tuned_warps(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
-    if (r->want_warps) return static_cast<int>(r->want_warps);
+// Autotuner: warps per CTA and visited-hash size for the persistent schedule,
+// picked per (dim, queue capacity) by timing each candidate on the first
+// call's batch (one warm and one timed launch each).
+Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
+    Tuning t;
+    if (r->want_warps && r->want_vh_bits && r->want_regs) {
+        t.warps = r->want_warps;
+        t.vh_bits = hash_bits_of(r->want_vh_bits);
+        t.regs = r->want_regs == 64 ? 1u : 0u;
+        return t;
+    }
     const uint64_t key = (static_cast<uint64_t>(r->idx->dim) << 32) | r->cap;
-    auto it = r->tuned_warps.find(key);
-    if (it != r->tuned_warps.end()) return static_cast<int>(it->second);
-    static const uint32_t candidates[] = {1, 2, 4, 8};
+    auto it = r->tuned.find(key);
+    if (it != r->tuned.end()) return it->second;
+    static const uint32_t warp_choices[] = {2, 4, 8};
+    static const uint32_t bit_choices[] = {0, 9, 10, 11};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     float best_ms = 1e30f;
-    uint32_t best = 4;
-    for (uint32_t w : candidates) {
-        LaunchShape s;
-        if (persistent_shape(r, w, &s) != ARTEA_GPU_OK) {
-            cudaGetLastError();
-            continue;
-        }
-        // One warm run, one timed run.
-        float ms = 0.f;
-        bool ok = true;
-        for (int rep = 0; rep < 2 && ok; ++rep) {
-            cudaEventRecord(e0, st);
-            ok = launch_with(r, a, true, w, st) == ARTEA_GPU_OK;
-            cudaEventRecord(e1, st);
-            ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
-        }
-        if (!ok) continue;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = w;
+    Tuning best;
+    best.warps = r->want_warps ? r->want_warps : 4;
+    best.vh_bits = r->want_vh_bits ? hash_bits_of(r->want_vh_bits) : 0;
+    for (uint32_t reg = 0; reg < 2; ++reg)
+    for (uint32_t w : warp_choices) {
+        if (r->want_regs && reg != (r->want_regs == 64 ? 1u : 0u)) continue;
+        if (r->want_warps && w != r->want_warps) continue;
+        for (uint32_t b : bit_choices) {
+            if (r->want_vh_bits && b != hash_bits_of(r->want_vh_bits)) continue;
+            Tuning c;
+            c.warps = w;
+            c.vh_bits = b;
+            c.regs = reg;
+            LaunchShape s;
+            if (persistent_shape(r, c, &s) != ARTEA_GPU_OK) {
+                cudaGetLastError();
+                continue;
+            }
+            float ms = 0.f;
+            bool ok = true;
+            for (int rep = 0; rep < 2 && ok; ++rep) {
+                cudaEventRecord(e0, st);
+                ok = launch_with(r, a, true, c, st) == ARTEA_GPU_OK;
+                cudaEventRecord(e1, st);
+                ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
+            }
+            if (!ok) {
+                cudaGetLastError();
+                continue;
+            }
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    r->tuned_warps[key] = best;
-    return static_cast<int>(best);
+    r->tuned[key] = best;
+    return best;
 }
 
 int check_kernel_error(artea_gpu_router* r) {
@@ -323,11 +381,12 @@ int run_device(artea_gpu_router* r, const float* d_q, uint32_t nq, const uint32_
     if (nq && (!d_q || !d_out)) return fail(ARTEA_GPU_EINVAL, "null query or output buffer");
     SearchArgs a;
     fill_args(r, &a, d_q, nq, d_topk, d_queue, k_stride, d_out, d_stats, l0_only);
-    bool persistent = r->schedule == ARTEA_GPU_SCHEDULE_PERSISTENT;
-    if (r->schedule == ARTEA_GPU_SCHEDULE_AUTO) persistent = true;
-    uint32_t warps = 1;
-    if (persistent) warps = static_cast<uint32_t>(tuned_warps(r, a, st));
-    return launch_with(r, a, persistent, warps, st);
+    bool persistent = r->schedule != ARTEA_GPU_SCHEDULE_PLAIN;
+    Tuning t;
+    t.warps = 1;
+    t.vh_bits = r->want_vh_bits ? hash_bits_of(r->want_vh_bits) : 0;
+    if (persistent) t = tuned(r, a, st);
+    return launch_with(r, a, persistent, t, st);
 }
 
 }  // namespace
@@ -406,7 +465,24 @@ int artea_gpu_index_create(const artea_gpu_graph_desc* g, const float* vectors, 
             ix->group_ptr[h] = ix->d_offsets + at;
             at += cnt;
         }
-        ix->bytes += sizeof(uint2) * ix->n + sizeof(uint32_t) * nn + sizeof(uint64_t) * total;
+        // Level-0 row descriptors (start | length << 40), one load per expansion.
+        if (g->num_neighbor_ids >= (1ull << kRowLenShift) || g->bl_max_nbr_size >= (1u << 24))
+            return cleanup(fail(ARTEA_GPU_EGRAPH, "graph too large for 40-bit row offsets"));
+        std::vector<unsigned long long> l0row(ix->n, 0ull);
+        for (uint32_t v = 0; v < ix->n; ++v) {
+            const uint32_t hl = g->vertex_info[2 * v];
+            if (hl == kInvalidLevel) continue;
+            const uint64_t local = g->vertex_info[2 * v + 1];
+            const uint64_t rrow = local * (hl + 1ull) + hl;
+            const uint64_t b = g->group_offsets[hl][rrow], e = g->group_offsets[hl][rrow + 1];
+            l0row[v] = b | ((e - b) << kRowLenShift);
+        }
+        if (int rc = dev_alloc(&ix->d_l0row, ix->n)) return cleanup(rc);
+        if (cudaMemcpy(ix->d_l0row, l0row.data(), sizeof(unsigned long long) * ix->n, cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+            return cleanup(fail(ARTEA_GPU_ECUDA, "row descriptor upload failed"));
+        ix->bytes += sizeof(uint2) * ix->n + sizeof(uint32_t) * nn + sizeof(uint64_t) * total +
+                     sizeof(unsigned long long) * ix->n;
     }
     *out = ix;
     return ARTEA_GPU_OK;
@@ -448,6 +524,7 @@ int artea_gpu_index_destroy(artea_gpu_index* ix) {
     dev_free(ix->d_vinfo);
     dev_free(ix->d_nbrs);
     dev_free(ix->d_offsets);
+    dev_free(ix->d_l0row);
     delete ix;
     return ARTEA_GPU_OK;
 }
@@ -473,7 +550,12 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
     if (o.metric < 0 || o.metric > 3) return fail(ARTEA_GPU_EINVAL, "unknown metric");
     if (o.mode != ARTEA_GPU_MODE_EXACT && o.mode != ARTEA_GPU_MODE_FAST) return fail(ARTEA_GPU_EINVAL, "unknown mode");
     if (o.schedule < 0 || o.schedule > 2) return fail(ARTEA_GPU_EINVAL, "unknown schedule");
-    if (o.warps_per_cta > 32) return fail(ARTEA_GPU_EINVAL, "warps_per_cta must be <= 32");
+    if (o.warps_per_cta > 8) return fail(ARTEA_GPU_EINVAL, "warps_per_cta must be <= 8");
+    if (o.register_budget != 0 && o.register_budget != 64 && o.register_budget != 85)
+        return fail(ARTEA_GPU_EINVAL, "register_budget must be 0 (autotuned), 64 or 85");
+    if (o.visited_hash_bits != 0 && o.visited_hash_bits != 0xffffffffu &&
+        (o.visited_hash_bits < 6 || o.visited_hash_bits > 12))
+        return fail(ARTEA_GPU_EINVAL, "visited_hash_bits must be 0 (autotuned), ~0 (no table) or in [6, 12]");
     DeviceGuard guard(ix->device);
     auto* r = new artea_gpu_router();
     r->idx = ix;
@@ -487,6 +569,8 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
     r->schedule = o.schedule;
     r->want_warps = o.warps_per_cta;
     r->want_ctas_per_sm = o.ctas_per_sm;
+    r->want_vh_bits = o.visited_hash_bits;
+    r->want_regs = o.register_budget;
     r->use_graphs = o.use_graphs != 0;
     r->words_per_slot = ((static_cast<uint64_t>(ix->n) + 127) / 128) * 4;   // multiple of 4 words
     r->list_cap = std::max<uint32_t>(std::min<uint32_t>(ix->n, 32768), 64);
@@ -586,6 +670,21 @@ int artea_gpu_router_sync(artea_gpu_router* r) {
     DeviceGuard guard(r->idx->device);
     CUDA_TRY(cudaDeviceSynchronize());
     return check_kernel_error(r);
+}
+
+int artea_gpu_router_set_phase_buffer(artea_gpu_router* r, void* d_phase_cycles) {
+    if (!r) return fail(ARTEA_GPU_EINVAL, "null router");
+    r->d_phase = static_cast<unsigned long long*>(d_phase_cycles);
+    return ARTEA_GPU_OK;
+}
+
+int artea_gpu_router_tuning(const artea_gpu_router* r, uint32_t* warps_per_cta, uint32_t* visited_hash_bits,
+                            uint32_t* register_budget) {
+    if (!r || !warps_per_cta || !visited_hash_bits || !register_budget) return fail(ARTEA_GPU_EINVAL, "null argument");
+    *warps_per_cta = r->last.warps;
+    *visited_hash_bits = r->last.vh_bits;
+    *register_budget = r->last.regs ? 64u : 85u;
+    return ARTEA_GPU_OK;
 }
 
 int artea_gpu_router_launches(const artea_gpu_router* r, uint64_t* launches) {

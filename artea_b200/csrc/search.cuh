@@ -12,11 +12,12 @@
 //   vinfo     N x {highest_level, local_vid} (uint2)
 //   offsets   per highest-level group h: N_h*(h+1)+1 uint64 CSR offsets
 //   nbrs      uint32 neighbour ids in CSR row order
-// Per search slot (one per resident warp):
-//   visited bitset (N bits) + visited list (ids set since the last clear)
+//   l0row     N x uint64 level-0 row descriptor: start | length << 40
+// Per search slot (one per resident warp): a spill bitset (N bits) and the
+// list of ids set in it since the last clear.
 //
 // Shared memory per warp: the query row, the candidate queue (sorted array of
-// (dist, vid|explored) with room for 2L entries) and a candidate batch.
+// (dist, vid|explored), 2L slots), a candidate batch and the visited hash.
 #pragma once
 
 #include <cstdint>
@@ -31,8 +32,11 @@ constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kExplored = 0x80000000u;
 constexpr uint32_t kVidMask = 0x7fffffffu;
 constexpr uint32_t kInvalidLevel = 0xffffffffu;
+constexpr uint32_t kEmptySlot = 0xffffffffu;
 constexpr uint32_t kCandBatch = 64;     // candidates evaluated per distance batch
 constexpr int kMaxGroups = 64;
+constexpr int kRowLenShift = 40;        // l0row: start in bits 0..39, length in 40..63
+constexpr unsigned long long kRowStartMask = (1ull << kRowLenShift) - 1ull;
 
 enum : int {
     kErrNone = 0,
@@ -46,6 +50,7 @@ struct DeviceGraph {
     const float* __restrict__ vecs;
     const uint2* __restrict__ vinfo;
     const uint32_t* __restrict__ nbrs;
+    const unsigned long long* __restrict__ l0row;
     uint32_t n;
     uint32_t dim;
     uint32_t top;      // kInvalidLevel when empty
@@ -63,6 +68,8 @@ struct SearchArgs {
     uint32_t queue_default;
     uint32_t k_stride;
     uint32_t cap;                         // queue entries per warp (>= 2 * max queue)
+    uint32_t vh_bits;                     // log2 of the shared-memory visited bucket count (0: none)
+    uint32_t vk_bits;                     // log2 of the vid permutation space (>= log2 N, > vh_bits)
     uint64_t* __restrict__ out;
     artea_gpu_query_stats* __restrict__ stats;   // may be null
     uint32_t* __restrict__ vis_bits;      // slots x words_per_slot
@@ -72,6 +79,20 @@ struct SearchArgs {
     uint32_t* __restrict__ next_query;    // persistent schedule work counter
     int* __restrict__ error;
     uint32_t l0_only;
+    unsigned long long* __restrict__ phase_cycles;   // nq x kPhases, optional
+};
+
+// Phase-cycle breakdown written per query when phase_cycles is set.
+enum : int {
+    kPhUpper = 0,     // greedy descent on levels >= 1
+    kPhPop = 1,       // pop, row descriptor, first ids, next-entry prefetch
+    kPhCollect = 2,   // row ids + visited test_and_set
+    kPhDist = 3,      // distance batches
+    kPhMerge = 4,     // queue merge
+    kPhTail = 5,      // result write-out and visited clear
+    kPhTotal = 6,     // whole query
+    kPhPrefetchHits = 7,  // expansions whose row descriptor was prefetched
+    kPhases = 8
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -134,7 +155,6 @@ __device__ float query_sqnorm(const float* __restrict__ q, uint32_t dim) {
     return fold16<kExact>(a0, a1, a2, a3);
 }
 
-// Distances for cnt candidates (ids in cvid, shared memory) into cdist.
 // Per pass each lane issues up to kBlock float4 loads of its row segment
 // before any arithmetic, so a D=128 row costs one memory round trip.
 constexpr int kBlock = 8;
@@ -157,6 +177,7 @@ __device__ __forceinline__ void accumulate(const float4 x, const float4 y, float
     }
 }
 
+// Distances for cnt candidates (ids in cvid, shared memory) into cdist.
 template <int kMetric, bool kExact>
 __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ q, float qsq,
                                 const uint32_t* cvid, float* cdist, uint32_t cnt) {
@@ -165,6 +186,14 @@ __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ 
     const int gi = lane & 3;
     const uint32_t dim = g.dim;
     const uint32_t nchunks = dim >> 4;
+    if (cnt > 8) {
+        // Rows of later passes: one bulk L2 prefetch per row, so those passes
+        // hit L2 instead of paying a full HBM round trip each.
+        for (uint32_t i = 8 + lane; i < cnt; i += 32) {
+            const float* rowp = g.vecs + static_cast<size_t>(cvid[i]) * dim;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rowp), "r"(dim * 4u) : "memory");
+        }
+    }
     for (uint32_t p = 0; p < cnt; p += 8) {
         const uint32_t idx = p + r;
         const bool valid = idx < cnt;
@@ -204,89 +233,150 @@ __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// Visited set (subsystem c): per-slot bitset in HBM; atomicOr gives
-// test_and_set (containers/version_tag_table.hpp:128-132). Every id set is
-// appended to the slot's list so clear() (a version bump in the reference,
-// version_tag_table.hpp:142-148) only zeroes the words it touched; if the list
-// overflows, the whole bitset is zeroed instead.
+// Visited set (subsystem c): exact, in two tiers.
+//   1. A bucketed table in shared memory. vid -> p = (vid * odd) mod 2^kbits is
+//      a bijection, so (bucket = high tbits bits of p, quotient = the other
+//      kbits - tbits bits) identifies vid exactly; a bucket is 8 uint16
+//      quotients (16 bytes), read with one vector load. 0xFFFF marks an
+//      empty slot (quotients have at most 15 bits).
+//   2. The slot's bitset in HBM (atomicOr = test_and_set,
+//      containers/version_tag_table.hpp:128-132), used for ids whose bucket is
+//      full. Buckets only fill up, never drain, until clear(): an id absent
+//      from a bucket that still has a free slot was never visited; only ids
+//      hashing to a full bucket need the bitset.
+// Ids set in the bitset are listed so clear() (a version bump in the
+// reference, version_tag_table.hpp:142-148) zeroes only the words it touched,
+// or the whole bitset if the list overflowed. With no table (tbits == 0)
+// every id goes to the bitset.
 // ---------------------------------------------------------------------------
+constexpr uint32_t kVisitedMul = 0x9E3779B1u;   // odd: multiplication mod 2^k is a bijection
+
 struct Visited {
+    uint4* tab;         // shared-memory buckets
+    uint32_t tbits;     // log2 of the bucket count (0: no table)
+    uint32_t kbits;     // log2 of the permutation space
+    uint32_t kmask;     // 2^kbits - 1
     uint32_t* bits;
     uint32_t* list;
     uint32_t list_n;
     uint32_t list_cap;
     uint64_t words;
-    bool spilled;
+    bool global_used;
+    bool list_overflow;
     uint32_t spills;
 };
 
-__device__ __forceinline__ void visited_record(Visited& vs, uint32_t vid, bool is_new) {
-    const int lane = lane_id();
-    const uint32_t b = __ballot_sync(kFull, is_new);
-    const uint32_t pos = vs.list_n + __popc(b & ((1u << lane) - 1u));
-    if (is_new) {
-        if (pos < vs.list_cap) vs.list[pos] = vid;
+// Returns 1 if vid is in its bucket, 0 if it was inserted now, 2 if its
+// bucket is full (the bitset decides).
+__device__ __forceinline__ int table_test_insert(const Visited& vs, uint32_t vid) {
+    const uint32_t p = (vid * kVisitedMul) & vs.kmask;
+    const uint32_t qbits = vs.kbits - vs.tbits;
+    const uint32_t bucket = p >> qbits;
+    const uint32_t quot = p & ((1u << qbits) - 1u);   // < 0x8000 by construction
+    const uint32_t pair = quot | (quot << 16);
+    uint32_t* w = reinterpret_cast<uint32_t*>(vs.tab + bucket);
+    for (int attempt = 0; attempt < 16; ++attempt) {
+        const uint4 b = vs.tab[bucket];
+        if (__vcmpeq2(b.x, pair) | __vcmpeq2(b.y, pair) | __vcmpeq2(b.z, pair) | __vcmpeq2(b.w, pair)) return 1;
+        const uint32_t e0 = __vcmpeq2(b.x, 0xFFFFFFFFu), e1 = __vcmpeq2(b.y, 0xFFFFFFFFu);
+        const uint32_t e2 = __vcmpeq2(b.z, 0xFFFFFFFFu), e3 = __vcmpeq2(b.w, 0xFFFFFFFFu);
+        int wi;
+        uint32_t old, e;
+        if (e0) { wi = 0; old = b.x; e = e0; }
+        else if (e1) { wi = 1; old = b.y; e = e1; }
+        else if (e2) { wi = 2; old = b.z; e = e2; }
+        else if (e3) { wi = 3; old = b.w; e = e3; }
+        else return 2;
+        const uint32_t desired = (e & 0xFFFFu) ? ((old & 0xFFFF0000u) | quot) : ((old & 0x0000FFFFu) | (quot << 16));
+        if (atomicCAS(w + wi, old, desired) == old) return 0;
+        // Another lane filled that slot meanwhile: read the bucket again.
     }
-    const uint32_t total = vs.list_n + __popc(b);
-    if (total > vs.list_cap) vs.spilled = true;
-    vs.list_n = min(total, vs.list_cap);
+    return 2;
+}
+
+// test_and_set for one id per lane (act lanes hold distinct vids); all lanes
+// call. Returns true in the lanes whose id was not yet visited.
+__device__ __forceinline__ bool visited_test_and_set(Visited& vs, uint32_t vid, bool act) {
+    const int lane = lane_id();
+    bool is_new = false;
+    bool in_bits = false;
+    if (act) {
+        const int t = vs.tbits ? table_test_insert(vs, vid) : 2;
+        if (t == 0) {
+            is_new = true;
+        } else if (t == 2) {
+            const uint32_t mask = 1u << (vid & 31);
+            const uint32_t old = atomicOr(vs.bits + (vid >> 5), mask);
+            is_new = !(old & mask);
+            in_bits = is_new;
+        }
+    }
+    const uint32_t b = __ballot_sync(kFull, in_bits);
+    if (b) {
+        const uint32_t pos = vs.list_n + __popc(b & ((1u << lane) - 1u));
+        if (in_bits && pos < vs.list_cap) vs.list[pos] = vid;
+        const uint32_t total = vs.list_n + __popc(b);
+        if (total > vs.list_cap) vs.list_overflow = true;
+        vs.list_n = min(total, vs.list_cap);
+        vs.global_used = true;
+    }
+    __syncwarp();
+    return is_new;
 }
 
 // set(): mark one id (all lanes call with the same vid).
 __device__ __forceinline__ void visited_set(Visited& vs, uint32_t vid) {
-    const int lane = lane_id();
-    bool is_new = false;
-    if (lane == 0) {
-        const uint32_t old = atomicOr(vs.bits + (vid >> 5), 1u << (vid & 31));
-        is_new = !(old & (1u << (vid & 31)));
+    visited_test_and_set(vs, vid, lane_id() == 0);
+}
+
+__device__ __forceinline__ void table_reset(const Visited& vs) {
+    if (vs.tbits) {
+        const uint32_t n = 1u << vs.tbits;
+        for (uint32_t i = lane_id(); i < n; i += 32) vs.tab[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
     }
-    visited_record(vs, vid, is_new);
 }
 
 __device__ void visited_clear(Visited& vs) {
     const int lane = lane_id();
     __syncwarp();
-    if (vs.spilled) {
-        uint4* w4 = reinterpret_cast<uint4*>(vs.bits);
-        const uint64_t n4 = vs.words / 4;
-        for (uint64_t i = lane; i < n4; i += 32) w4[i] = make_uint4(0, 0, 0, 0);
+    table_reset(vs);
+    if (vs.global_used) {
+        if (vs.list_overflow) {
+            uint4* w4 = reinterpret_cast<uint4*>(vs.bits);
+            const uint64_t n4 = vs.words / 4;
+            for (uint64_t i = lane; i < n4; i += 32) w4[i] = make_uint4(0, 0, 0, 0);
+        } else {
+            for (uint32_t i = lane; i < vs.list_n; i += 32) vs.bits[vs.list[i] >> 5] = 0u;
+        }
         vs.spills++;
-    } else {
-        for (uint32_t i = lane; i < vs.list_n; i += 32) vs.bits[vs.list[i] >> 5] = 0u;
     }
     vs.list_n = 0;
-    vs.spilled = false;
+    vs.global_used = false;
+    vs.list_overflow = false;
     __threadfence_block();
     __syncwarp();
 }
 
-// Collect the not-yet-visited ids of row[0, len) (CSR order, first occurrence
-// wins, marking them visited) into cvid[0, *cnt). Returns false on a bad id.
-// Processes at most kCandBatch new ids; *consumed reports how far it got.
-__device__ bool collect_unvisited(const DeviceGraph& g, Visited& vs, const uint32_t* __restrict__ row,
-                                  uint32_t len, uint32_t start, uint32_t* cvid, uint32_t* cnt,
-                                  uint32_t* consumed, int* error) {
+// Collect the not-yet-visited ids of row[start, len) (CSR order, first
+// occurrence wins, marking them visited) into cvid[0, *cnt), at most
+// kCandBatch of them; *consumed reports how far it got. The ids of row[0, 32)
+// and row[32, 64) may be passed in preloaded (ids0/ids1, one per lane).
+__device__ __forceinline__ void collect_unvisited(const DeviceGraph& g, Visited& vs, const uint32_t* __restrict__ row,
+                                                  uint32_t len, uint32_t start, uint32_t* cvid, uint32_t* cnt,
+                                                  uint32_t* consumed, int* error, uint32_t ids0, uint32_t ids1,
+                                                  bool have_ids) {
     const int lane = lane_id();
     uint32_t c = 0;
     uint32_t i = start;
-    bool ok = true;
     while (i < len && c + 32 <= kCandBatch) {
         const uint32_t idx = i + lane;
         const bool act = idx < len;
-        uint32_t vid = act ? __ldg(row + idx) : 0xffffffffu;
-        if (act && vid >= g.n) {
-            set_error(error, kErrBadVid);
-            ok = false;
-        }
+        uint32_t vid = 0xffffffffu;
+        if (act) vid = (have_ids && i == 0) ? ids0 : (have_ids && i == 32) ? ids1 : __ldg(row + idx);
+        if (act && vid >= g.n) set_error(error, kErrBadVid);
         const uint32_t peers = __match_any_sync(kFull, vid);
         const bool first = act && ((peers & ((1u << lane) - 1u)) == 0) && vid < g.n;
-        bool is_new = false;
-        if (first) {
-            const uint32_t mask = 1u << (vid & 31);
-            const uint32_t old = atomicOr(vs.bits + (vid >> 5), mask);
-            is_new = !(old & mask);
-        }
-        visited_record(vs, vid, is_new);
+        const bool is_new = visited_test_and_set(vs, vid, first);
         const uint32_t b = __ballot_sync(kFull, is_new);
         if (is_new) cvid[c + __popc(b & ((1u << lane) - 1u))] = vid;
         c += __popc(b);
@@ -295,7 +385,6 @@ __device__ bool collect_unvisited(const DeviceGraph& g, Visited& vs, const uint3
     __syncwarp();
     *cnt = c;
     *consumed = min(i, len);
-    return __all_sync(kFull, ok);
 }
 
 // ---------------------------------------------------------------------------
@@ -373,64 +462,143 @@ __device__ __forceinline__ bool queue_insert(Queue& q, float d, uint32_t v, int*
     return true;
 }
 
+// First unexplored entry at or after `from`, or -1.
+__device__ __forceinline__ int queue_find_unexplored(const Queue& q, uint32_t from) {
+    const int lane = lane_id();
+    for (uint32_t base = from; base < q.n; base += 32) {
+        const uint32_t idx = base + lane;
+        const bool un = idx < q.n && !(q.v[idx] & kExplored);
+        const uint32_t b = __ballot_sync(kFull, un);
+        if (b) return static_cast<int>(base + __ffs(b) - 1);
+    }
+    return -1;
+}
+
 // pop_best_unexplored_entry + should_terminate (std_candidate_queue.hpp:398-406,
 // 503-513): the first unexplored entry in order, or -1 when the reference's
 // unexplored heap holds nothing at distance <= lb.
 __device__ __forceinline__ int queue_pop(Queue& q) {
-    const int lane = lane_id();
-    for (uint32_t base = q.hint; base < q.n; base += 32) {
-        const uint32_t idx = base + lane;
-        const bool un = idx < q.n && !(q.v[idx] & kExplored);
-        const uint32_t b = __ballot_sync(kFull, un);
-        if (b) {
-            const uint32_t p = base + __ffs(b) - 1;
-            if (lane == 0) q.v[p] |= kExplored;
-            __syncwarp();
-            q.hint = p + 1;
-            return static_cast<int>(p);
-        }
+    const int p = queue_find_unexplored(q, q.hint);
+    if (p < 0) {
+        q.hint = q.n;
+        return -1;
     }
-    q.hint = q.n;
-    return -1;
+    if (lane_id() == 0) q.v[p] |= kExplored;
+    __syncwarp();
+    q.hint = static_cast<uint32_t>(p) + 1;
+    return p;
 }
 
-// try_push for a batch, in candidate order (std_candidate_queue.hpp:358-388):
-// reject when T is full and d >= lb, else insert.
-__device__ __forceinline__ void queue_push_batch_exact(Queue& q, const uint32_t* cvid, const float* cdist,
-                                                       uint32_t cnt, int* error) {
+// try_push for a whole batch at once (std_candidate_queue.hpp:358-388).
+// Sequentially, candidate j is rejected iff T already holds L entries at
+// distance <= d_j. A rejected candidate never enters T, and every later
+// candidate at a distance >= a rejected one is rejected too, so candidate j
+// is accepted iff
+//     #{e in T : e.dist <= d_j} + #{i < j : d_i <= d_j}  <  L,
+// which every lane evaluates independently. The accepted candidates are then
+// merged into the sorted array in one pass; trimming the result at the new
+// lb yields exactly the state the sequential pushes leave (entries trimmed
+// in between are worse than every later lb).
+// Scratch: bd/bv hold the accepted batch; cdist/cvid are reused for its
+// sorted copy.
+__device__ void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, uint32_t cnt, float* bd, uint32_t* bv,
+                                 int* error) {
     const int lane = lane_id();
-    uint32_t i = 0;
-    while (i < cnt) {
-        uint32_t j;
-        if (q.n < q.L) {
-            j = i;
-        } else {
-            j = 0xffffffffu;
-            for (uint32_t base = i; base < cnt; base += 32) {
-                const uint32_t idx = base + lane;
-                const bool acc = idx < cnt && cdist[idx] < q.lb;
-                const uint32_t b = __ballot_sync(kFull, acc);
-                if (b) { j = base + __ffs(b) - 1; break; }
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t tn = min(q.n, q.L);
+    uint32_t m = 0;
+    for (uint32_t base = 0; base < cnt; base += 32) {
+        const uint32_t j = base + lane;
+        bool acc = false;
+        float d = 0.f;
+        uint32_t v = 0;
+        if (j < cnt) {
+            d = cdist[j];
+            v = cvid[j];
+            uint32_t lo = 0, hi = tn;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (q.d[mid] <= d) lo = mid + 1; else hi = mid;
             }
-            if (j == 0xffffffffu) break;
+            uint32_t pre = 0;
+            for (uint32_t i = 0; i < j; ++i) pre += cdist[i] <= d ? 1u : 0u;
+            acc = lo + pre < q.L;
         }
-        if (!queue_insert(q, cdist[j], cvid[j], error)) return;
-        i = j + 1;
+        const uint32_t b = __ballot_sync(kFull, acc);
+        if (acc) {
+            const uint32_t k = m + __popc(b & lt_mask);
+            bd[k] = d;
+            bv[k] = v;
+        }
+        m += __popc(b);
     }
-}
-
-// FAST-mode merge: every candidate better than the current lb (or any while T
-// is not full) is inserted in one pass per candidate without re-testing
-// against the lb it lowers; ties are then ordered by vid.
-__device__ __forceinline__ void queue_push_batch_fast(Queue& q, const uint32_t* cvid, const float* cdist,
-                                                      uint32_t cnt, int* error) {
-    const float lb0 = q.n >= q.L ? q.lb : FLT_MAX;
-    for (uint32_t j = 0; j < cnt; ++j) {
-        const float d = cdist[j];
-        if (q.n >= q.L && !(d < q.lb)) continue;
-        if (!(d < lb0) && q.n >= q.L) continue;
-        if (!queue_insert(q, d, cvid[j], error)) return;
+    __syncwarp();
+    if (m == 0) return;
+    // Sort the accepted batch by (dist, vid) into cdist/cvid (ranks are unique).
+    for (uint32_t k = lane; k < m; k += 32) {
+        const float d = bd[k];
+        const uint32_t v = bv[k];
+        uint32_t r = 0;
+        for (uint32_t i = 0; i < m; ++i) r += entry_less(bd[i], bv[i], d, v) ? 1u : 0u;
+        cdist[r] = d;
+        cvid[r] = v;
     }
+    __syncwarp();
+    // Final positions of the batch entries: rank in the old array + rank in the batch.
+    uint32_t posb[2] = {0xffffffffu, 0xffffffffu};
+    for (uint32_t r = lane, t = 0; r < m; r += 32, ++t) {
+        const float d = cdist[r];
+        const uint32_t v = cvid[r];
+        uint32_t lo = 0, hi = q.n;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (entry_less(q.d[mid], q.v[mid], d, v)) lo = mid + 1; else hi = mid;
+        }
+        posb[t] = lo + r;
+    }
+    const uint32_t p0 = __shfl_sync(kFull, posb[0], 0);   // position of the smallest batch entry
+    // Move the old entries from p0 on to the right by the number of batch
+    // entries smaller than them, tail first (targets never overlap unread ones).
+    for (int end = static_cast<int>(q.n); end > static_cast<int>(p0); end -= 32) {
+        const int s0 = max(static_cast<int>(p0), end - 32);
+        const int i = s0 + lane;
+        const bool act = i < end;
+        float dd = 0.f;
+        uint32_t vv = 0;
+        uint32_t np = 0xffffffffu;
+        if (act) {
+            dd = q.d[i];
+            vv = q.v[i];
+            uint32_t lo = 0, hi = m;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (entry_less(cdist[mid], cvid[mid], dd, vv)) lo = mid + 1; else hi = mid;
+            }
+            np = static_cast<uint32_t>(i) + lo;
+        }
+        __syncwarp();
+        if (act && np < q.cap) { q.d[np] = dd; q.v[np] = vv; }
+        __syncwarp();
+    }
+    for (uint32_t r = lane, t = 0; r < m; r += 32, ++t) {
+        if (posb[t] < q.cap) { q.d[posb[t]] = cdist[r]; q.v[posb[t]] = cvid[r] & kVidMask; }
+    }
+    __syncwarp();
+    const uint32_t total = min(q.n + m, q.cap);
+    q.n = total;
+    if (p0 < q.hint) q.hint = p0;
+    if (q.n >= q.L) {
+        q.lb = q.d[q.L - 1];
+        uint32_t newn = q.n;
+        for (uint32_t base = q.L; base < q.n; base += 32) {
+            const uint32_t idx = base + lane;
+            const bool dead = idx < q.n && q.d[idx] > q.lb;
+            const uint32_t b = __ballot_sync(kFull, dead);
+            if (b) { newn = base + __ffs(b) - 1; break; }
+        }
+        q.n = newn;
+    }
+    (void)error;
 }
 
 // ---------------------------------------------------------------------------
@@ -456,12 +624,71 @@ struct Counters {
     uint32_t dist_evals, upper_rows, upper_row_ids, l0_rows, l0_row_ids, upper_dist_evals;
 };
 
+// Accumulates clock64() deltas per phase when enabled (warp-uniform flag);
+// the accumulators live in the warp's shared memory, lane 0 updates them.
+struct PhaseClock {
+    bool on;
+    long long t;
+    unsigned long long* acc;
+    __device__ __forceinline__ void start(bool enabled, unsigned long long* smem_acc) {
+        on = enabled;
+        acc = smem_acc;
+        if (on) {
+            if (lane_id() < kPhases) acc[lane_id()] = 0;
+            __syncwarp();
+            t = clock64();
+        }
+    }
+    __device__ __forceinline__ void lap(int phase) {
+        if (on) {
+            const long long now = clock64();
+            if (lane_id() == 0) acc[phase] += static_cast<unsigned long long>(now - t);
+            t = now;
+        }
+    }
+    __device__ __forceinline__ void count(int phase) {
+        if (on && lane_id() == 0) acc[phase] += 1;
+    }
+};
+
+// Shared memory words per warp for a launch.
+constexpr uint32_t kPhaseWords = 2 * kPhases;   // kPhases uint64 accumulators
+
+__host__ __device__ inline uint32_t warp_smem_words(uint32_t dim, uint32_t cap, uint32_t vh_bits) {
+    return dim + 2 * cap + 4 * kCandBatch + (vh_bits ? 4u * (1u << vh_bits) : 0u) + kPhaseWords;
+}
+
+struct WarpSmem {
+    unsigned long long* phase;   // kPhases accumulators (8-byte aligned: first)
+    float* q;
+    float* qd;
+    uint32_t* qv;
+    uint32_t* cvid;
+    float* cdist;
+    float* bd;
+    uint32_t* bv;
+    uint32_t* vh;
+};
+
+__device__ __forceinline__ WarpSmem carve(float* base, uint32_t dim, uint32_t cap) {
+    WarpSmem s;
+    s.phase = reinterpret_cast<unsigned long long*>(base);
+    s.q = base + kPhaseWords;
+    s.qd = s.q + dim;
+    s.qv = reinterpret_cast<uint32_t*>(s.qd + cap);
+    s.cvid = s.qv + cap;
+    s.cdist = reinterpret_cast<float*>(s.cvid + kCandBatch);
+    s.bd = s.cdist + kCandBatch;
+    s.bv = reinterpret_cast<uint32_t*>(s.bd + kCandBatch);
+    s.vh = s.bv + kCandBatch;
+    return s;
+}
+
 // ---------------------------------------------------------------------------
 // One query (hierarchical_graph_router.hpp:195-248; query_l0_only :258-286).
 // ---------------------------------------------------------------------------
 template <int kMetric, bool kExact>
-__device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, float* smem_q, float* qd, uint32_t* qv,
-                           uint32_t* cvid, float* cdist) {
+__device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, const WarpSmem& sm) {
     const int lane = lane_id();
     const DeviceGraph& g = a.g;
     const uint32_t dim = g.dim;
@@ -478,28 +705,39 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, floa
 
     Counters ct = {};
     uint32_t nres = 0;
+    PhaseClock pc;
+    pc.start(a.phase_cycles != nullptr, sm.phase);
+    const long long t_begin = pc.on ? clock64() : 0;
     Visited vs;
+    vs.tab = reinterpret_cast<uint4*>(sm.vh);
+    vs.tbits = a.vh_bits;
+    vs.kbits = a.vk_bits;
+    vs.kmask = a.vk_bits >= 32 ? 0xFFFFFFFFu : ((1u << a.vk_bits) - 1u);
     vs.bits = a.vis_bits + static_cast<size_t>(slot) * a.words_per_slot;
     vs.list = a.vis_list + static_cast<size_t>(slot) * a.list_cap;
     vs.list_n = 0;
     vs.list_cap = a.list_cap;
     vs.words = a.words_per_slot;
-    vs.spilled = false;
+    vs.global_used = false;
+    vs.list_overflow = false;
     vs.spills = 0;
+    uint32_t* cvid = sm.cvid;
+    float* cdist = sm.cdist;
 
     if (g.n != 0 && g.top != kInvalidLevel && L > 0) {
-        // Stage the query row in shared memory.
+        // Stage the query row in shared memory; reset the visited hash.
         const float4* src = reinterpret_cast<const float4*>(a.queries + static_cast<size_t>(qi) * dim);
-        float4* dst = reinterpret_cast<float4*>(smem_q);
+        float4* dst = reinterpret_cast<float4*>(sm.q);
         for (uint32_t i = lane; i < dim / 4; i += 32) dst[i] = __ldg(src + i);
+        table_reset(vs);
         __syncwarp();
-        const float qsq = (kMetric == ARTEA_GPU_COSINE) ? query_sqnorm<kExact>(smem_q, dim) : 0.f;
+        const float qsq = (kMetric == ARTEA_GPU_COSINE) ? query_sqnorm<kExact>(sm.q, dim) : 0.f;
 
         // Entry point distance (hierarchical_graph_router.hpp:209-211).
         uint32_t cur = g.entry;
         if (lane == 0) cvid[0] = cur;
         __syncwarp();
-        batch_distances<kMetric, kExact>(g, smem_q, qsq, cvid, cdist, 1);
+        batch_distances<kMetric, kExact>(g, sm.q, qsq, cvid, cdist, 1);
         float cur_d = cdist[0];
         ct.dist_evals = 1;
 
@@ -518,10 +756,10 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, floa
                     uint32_t pos = 0;
                     while (pos < len) {
                         uint32_t cnt, consumed;
-                        collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error);
+                        collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error, 0u, 0u, false);
                         pos = consumed;
                         if (cnt == 0) continue;
-                        batch_distances<kMetric, kExact>(g, smem_q, qsq, cvid, cdist, cnt);
+                        batch_distances<kMetric, kExact>(g, sm.q, qsq, cvid, cdist, cnt);
                         ct.dist_evals += cnt;
                         ct.upper_dist_evals += cnt;
                         // First strict improvement in row order (beam_loop.hpp:153-160).
@@ -549,11 +787,12 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, floa
                 visited_clear(vs);
             }
         }
+        pc.lap(kPhUpper);
 
         // Level-0 beam search (single_layer_router.hpp:145-163, beam_loop.hpp:90-119).
         Queue q;
-        q.d = qd;
-        q.v = qv;
+        q.d = sm.qd;
+        q.v = sm.qv;
         q.n = 0;
         q.L = L;
         q.cap = a.cap;
@@ -561,27 +800,65 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, floa
         q.lb = FLT_MAX;
         queue_insert(q, cur_d, cur, a.error);
         visited_set(vs, cur);
+        // Software pipeline: while one row is processed, the row descriptor and
+        // then the neighbour ids of the entry that would be expanded next are
+        // already being loaded (used if that entry is indeed popped next).
+        uint32_t pf_vid = cur;
+        unsigned long long pf_desc = __ldg(g.l0row + cur);
+        uint32_t pf_ids0 = 0u, pf_ids1 = 0u;
+        bool pf_have_ids = false;
         for (uint32_t it = 0;; ++it) {
             if (it > g.n) { set_error(a.error, kErrBound); break; }
             const int p = queue_pop(q);
             if (p < 0) break;
             const uint32_t v = q.v[p] & kVidMask;
             if (v == kVidMask) break;   // CandidateEntry::is_invalid
-            uint32_t len;
-            const uint32_t* row = level_row(g, v, 0, &len);
+            const bool hit = v == pf_vid;
+            if (hit) pc.count(kPhPrefetchHits);
+            const unsigned long long desc = hit ? pf_desc : __ldg(g.l0row + v);
+            const uint32_t len = static_cast<uint32_t>(desc >> kRowLenShift);
+            const uint32_t* row = g.nbrs + (desc & kRowStartMask);
+            uint32_t ids0, ids1;
+            if (hit && pf_have_ids) {
+                ids0 = pf_ids0;
+                ids1 = pf_ids1;
+            } else {
+                ids0 = lane < len ? __ldg(row + lane) : 0xffffffffu;
+                ids1 = lane + 32 < len ? __ldg(row + lane + 32) : 0xffffffffu;
+            }
+            const int p2 = queue_find_unexplored(q, q.hint);
+            pf_have_ids = false;
+            if (p2 >= 0) {
+                pf_vid = q.v[p2] & kVidMask;
+                pf_desc = __ldg(g.l0row + pf_vid);
+            } else {
+                pf_vid = kVidMask;
+            }
             ct.l0_rows++;
             ct.l0_row_ids += len;
+            pc.lap(kPhPop);
             uint32_t pos = 0;
             while (pos < len) {
                 uint32_t cnt, consumed;
-                collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error);
+                collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error, ids0, ids1, pos == 0);
                 pos = consumed;
+                pc.lap(kPhCollect);
                 if (cnt == 0) continue;
-                batch_distances<kMetric, kExact>(g, smem_q, qsq, cvid, cdist, cnt);
+                batch_distances<kMetric, kExact>(g, sm.q, qsq, cvid, cdist, cnt);
                 ct.dist_evals += cnt;
-                if (kExact) queue_push_batch_exact(q, cvid, cdist, cnt, a.error);
-                else queue_push_batch_fast(q, cvid, cdist, cnt, a.error);
+                pc.lap(kPhDist);
+                if (p2 >= 0 && !pf_have_ids) {
+                    // The next entry's descriptor has arrived by now: fetch its ids
+                    // while the merge runs.
+                    const uint32_t len2 = static_cast<uint32_t>(pf_desc >> kRowLenShift);
+                    const uint32_t* row2 = g.nbrs + (pf_desc & kRowStartMask);
+                    pf_ids0 = lane < len2 ? __ldg(row2 + lane) : 0xffffffffu;
+                    pf_ids1 = lane + 32 < len2 ? __ldg(row2 + lane + 32) : 0xffffffffu;
+                    pf_have_ids = true;
+                }
+                queue_push_batch(q, cvid, cdist, cnt, sm.bd, sm.bv, a.error);
                 __syncwarp();
+                pc.lap(kPhMerge);
             }
         }
         visited_clear(vs);
@@ -592,7 +869,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, floa
         for (uint32_t i = lane; i < a.k_stride; i += 32) {
             uint64_t w = kInvalidWord;
             if (i < nres) {
-                w = (static_cast<uint64_t>(__float_as_uint(qd[i])) << 32) | (qv[i] & kVidMask);
+                w = (static_cast<uint64_t>(__float_as_uint(sm.qd[i])) << 32) | (sm.qv[i] & kVidMask);
             }
             out[i] = w;
         }
@@ -600,6 +877,12 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, floa
         for (uint32_t i = lane; i < a.k_stride; i += 32) out[i] = kInvalidWord;
     }
 
+    pc.lap(kPhTail);
+    if (pc.on) {
+        if (lane == 0) pc.acc[kPhTotal] = static_cast<unsigned long long>(clock64() - t_begin);
+        __syncwarp();
+        if (lane < kPhases) a.phase_cycles[static_cast<size_t>(qi) * kPhases + lane] = pc.acc[lane];
+    }
     if (a.stats && lane == 0) {
         artea_gpu_query_stats s;
         s.dist_evals = ct.dist_evals;
@@ -615,43 +898,33 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, floa
     __syncwarp();
 }
 
-// Shared memory floats per warp for a launch.
-__host__ __device__ inline uint32_t warp_smem_words(uint32_t dim, uint32_t cap) {
-    return dim + 2 * cap + 2 * kCandBatch;
-}
-
-// Plain schedule: one CTA of one warp per query; slot = query index.
+// Plain schedule: one CTA of one warp per query; slot = query index
+// (24 resident CTAs per SM at the 85-register budget).
 template <int kMetric, bool kExact>
-__global__ void __launch_bounds__(32) search_plain_kernel(SearchArgs a) {
+__global__ void __launch_bounds__(32, 24) search_plain_kernel(SearchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const uint32_t qi = blockIdx.x;
     if (qi >= a.nq) return;
-    float* smem_q = smem;
-    float* qd = smem_q + a.g.dim;
-    uint32_t* qv = reinterpret_cast<uint32_t*>(qd + a.cap);
-    uint32_t* cvid = qv + a.cap;
-    float* cdist = reinterpret_cast<float*>(cvid + kCandBatch);
-    search_one<kMetric, kExact>(a, qi, qi, smem_q, qd, qv, cvid, cdist);
+    const WarpSmem sm = carve(smem, a.g.dim, a.cap);
+    search_one<kMetric, kExact>(a, qi, qi, sm);
 }
 
 // Persistent schedule: warps pull query indices from a shared counter.
-template <int kMetric, bool kExact>
-__global__ void search_persistent_kernel(SearchArgs a) {
+// kMinBlocks sets the register budget: 4 blocks of 256 threads per SM caps a
+// thread at 64 registers (32 resident warps), 3 at 85 (24 warps).
+template <int kMetric, bool kExact, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) search_persistent_kernel(SearchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
-    float* base = smem + static_cast<size_t>(warp) * warp_smem_words(a.g.dim, a.cap);
-    float* smem_q = base;
-    float* qd = smem_q + a.g.dim;
-    uint32_t* qv = reinterpret_cast<uint32_t*>(qd + a.cap);
-    uint32_t* cvid = qv + a.cap;
-    float* cdist = reinterpret_cast<float*>(cvid + kCandBatch);
+    const WarpSmem sm = carve(smem + static_cast<size_t>(warp) * warp_smem_words(a.g.dim, a.cap, a.vh_bits),
+                              a.g.dim, a.cap);
     for (;;) {
         uint32_t qi = 0;
         if (lane_id() == 0) qi = atomicAdd(a.next_query, 1u);
         qi = __shfl_sync(kFull, qi, 0);
         if (qi >= a.nq) break;
-        search_one<kMetric, kExact>(a, qi, slot, smem_q, qd, qv, cvid, cdist);
+        search_one<kMetric, kExact>(a, qi, slot, sm);
     }
 }
 

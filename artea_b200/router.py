@@ -112,7 +112,7 @@ class GpuRouter:
 
     def __init__(self, index: DeviceIndex, metric, topk: int, candidate_queue_size: int, mode: str = "exact",
                  schedule: str = "auto", warps_per_cta: int = 0, ctas_per_sm: int = 0, max_batch: int = 0,
-                 max_queue: int = 0):
+                 max_queue: int = 0, visited_hash_bits: int = 0, register_budget: int = 0):
         opts = nat.RouterOpts()
         opts.metric = metric_code(metric)
         opts.mode = MODES[mode] if isinstance(mode, str) else int(mode)
@@ -121,6 +121,8 @@ class GpuRouter:
         opts.ctas_per_sm = ctas_per_sm
         opts.max_batch = max_batch
         opts.max_queue = max_queue
+        opts.visited_hash_bits = visited_hash_bits
+        opts.register_budget = register_budget
         h = ctypes.c_void_p()
         nat.check(nat.lib().artea_gpu_router_create(index.handle, topk, candidate_queue_size, ctypes.byref(opts),
                                                     ctypes.byref(h)))
@@ -169,6 +171,16 @@ class GpuRouter:
 
     def sync(self) -> None:
         nat.check(nat.lib().artea_gpu_router_sync(self._h))
+
+    def set_phase_buffer(self, d_buf) -> None:
+        """Record per-query phase cycles into d_buf (device, nq x 8 int64) or stop (None)."""
+        nat.check(nat.lib().artea_gpu_router_set_phase_buffer(self._h, nat.ptr(d_buf)))
+
+    def tuning(self) -> dict:
+        """Launch parameters of the last launch (the autotuner's pick)."""
+        w, b, g = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        nat.check(nat.lib().artea_gpu_router_tuning(self._h, ctypes.byref(w), ctypes.byref(b), ctypes.byref(g)))
+        return {"warps_per_cta": w.value, "visited_hash_bits": b.value, "register_budget": g.value}
 
     def launches(self) -> int:
         n = ctypes.c_uint64()

@@ -14,7 +14,9 @@ import fcntl
 import json
 import os
 import subprocess
+import sys
 import time
+import zlib
 from typing import Optional, Tuple
 
 import numpy as np
@@ -24,6 +26,9 @@ from . import datasets as ds
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BUILDER = os.path.join(ROOT, "index_build", "_ref", "artea_build_index")
 DEFAULT_CACHE = os.environ.get("ARTEA_CACHE", os.path.join(ROOT, ".cache"))
+# zlib-compressed snapshots built elsewhere by the same builder for the same
+# vectors (same file stem = same vector fingerprint); used instead of a build.
+PREBUILT = os.path.join(ROOT, "prebuilt")
 
 BUILD_PARAMS = dict(beta=2.0, tau_k=0.0, tau=1.5, search_nn_qs=64, loops=15, triu=4, prefill=0.4, scale=1.10,
                     shift=1.5, shuffle=1)
@@ -44,6 +49,17 @@ def graph_for(base: np.ndarray, metric: str, l0: float = 1.0, cache_dir: Optiona
         if os.path.exists(hgra) and os.path.exists(meta):
             with open(meta) as f:
                 return hgra, json.load(f)
+        packed = os.path.join(PREBUILT, os.path.basename(stem))
+        if os.path.exists(packed + ".hgra.z") and os.path.exists(packed + ".json"):
+            _unpack(packed + ".hgra.z", hgra)
+            with open(packed + ".json") as f:
+                report = json.load(f)
+            report["prebuilt"] = True
+            with open(meta, "w") as f:
+                json.dump(report, f)
+            if log:
+                log(f"graph restored from {packed}.hgra.z (built by the reference builder on the same vectors)")
+            return hgra, report
         if not os.path.exists(BUILDER):
             raise FileNotFoundError(f"{BUILDER} is missing: build it with `make -C index_build` where the "
                                     "reference headers are available")
@@ -70,6 +86,37 @@ def graph_for(base: np.ndarray, metric: str, l0: float = 1.0, cache_dir: Optiona
         lock.close()
 
 
+def _unpack(src: str, dst: str) -> None:
+    d = zlib.decompressobj()
+    tmp = dst + ".tmp"
+    with open(src, "rb") as fi, open(tmp, "wb") as fo:
+        while True:
+            chunk = fi.read(1 << 24)
+            if not chunk:
+                break
+            fo.write(d.decompress(chunk))
+        fo.write(d.flush())
+    os.replace(tmp, dst)
+
+
+def export_prebuilt(hgra: str, meta: str, level: int = 6) -> str:
+    """Compress a cached snapshot into prebuilt/ under the same stem."""
+    os.makedirs(PREBUILT, exist_ok=True)
+    stem = os.path.join(PREBUILT, os.path.basename(hgra)[: -len(".hgra")])
+    c = zlib.compressobj(level)
+    with open(hgra, "rb") as fi, open(stem + ".hgra.z.tmp", "wb") as fo:
+        while True:
+            chunk = fi.read(1 << 24)
+            if not chunk:
+                break
+            fo.write(c.compress(chunk))
+        fo.write(c.flush())
+    os.replace(stem + ".hgra.z.tmp", stem + ".hgra.z")
+    with open(meta) as f, open(stem + ".json", "w") as g:
+        g.write(f.read())
+    return stem + ".hgra.z"
+
+
 def prepare(name: str, n_base: Optional[int] = None, n_query: Optional[int] = None, cache_dir: Optional[str] = None,
             log=None):
     """(workload, base, queries, hgra_path, build_report) for a named workload."""
@@ -79,3 +126,14 @@ def prepare(name: str, n_base: Optional[int] = None, n_query: Optional[int] = No
     base, queries = ds.generate(w)
     hgra, report = graph_for(base, w.metric, l0=w.l0_min_distance, cache_dir=cache_dir, tag=w.name, log=log)
     return w, base, queries, hgra, report
+
+
+if __name__ == "__main__":
+    # python -m artea_b200.workload build|export NAME [n_base n_query]
+    cmd, name = sys.argv[1], sys.argv[2]
+    nb = int(sys.argv[3]) if len(sys.argv) > 3 else None
+    nq = int(sys.argv[4]) if len(sys.argv) > 4 else None
+    w, base, queries, hgra, report = prepare(name, nb, nq, log=print)
+    print(hgra, report)
+    if cmd == "export":
+        print(export_prebuilt(hgra, hgra[: -len(".hgra")] + ".json"))

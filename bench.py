@@ -283,6 +283,14 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-queue", type=int, default=0)
     ap.add_argument("--reference-sample", type=int, default=2000)
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run: one warm and one measured launch at --profile-queue with "
+                         "--profile-warps warps per CTA; no sweep, ground truth or baseline")
+    ap.add_argument("--profile-queue", type=int, default=200)
+    ap.add_argument("--profile-warps", type=int, default=4)
+    ap.add_argument("--profile-vh-bits", type=int, default=-1, help="-1: no shared-memory visited hash")
+    ap.add_argument("--profile-regs", type=int, default=85)
+    ap.add_argument("--phases", action="store_true", help="with --profile: per-phase cycle breakdown")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -312,6 +320,36 @@ def main() -> None:
     graph = CompactHierarchicalGraph.from_hgra(hgra)
     index = DeviceIndex(graph, base, device=local)
     cache_dir = wl.DEFAULT_CACHE
+    if args.profile:
+        d_q = torch.from_numpy(queries).to(device)
+        d_out = torch.empty((nq, k), dtype=torch.int64, device=device)
+        r = GpuRouter(index, metric, k, args.profile_queue, mode=args.mode,
+                      schedule="plain" if args.schedule == "plain" else "persistent",
+                      warps_per_cta=args.profile_warps,
+                      visited_hash_bits=args.profile_vh_bits if args.profile_vh_bits >= 0 else 0xFFFFFFFF,
+                      register_budget=args.profile_regs, max_batch=nq)
+        s = torch.cuda.current_stream(device)
+        phases = torch.zeros((nq, 8), dtype=torch.int64, device=device) if args.phases else None
+        for rep in range(2):
+            if phases is not None and rep == 1:
+                r.set_phase_buffer(phases)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            r.batch_query_device(d_q, nq, k, d_out, stream=s.cuda_stream)
+            e1.record(s)
+            torch.cuda.synchronize(device)
+            log(f"profile launch: {e0.elapsed_time(e1):.3f} ms for {nq} queries")
+        r.sync()
+        if phases is not None:
+            ph = phases.cpu().numpy().astype(np.float64)
+            names = ["upper", "pop_row", "ids_visited", "distances", "merge", "tail", "total", "prefetch_hits"]
+            mean = ph.mean(axis=0)
+            print(json.dumps({"phase_cycles_mean": dict(zip(names, mean.tolist())),
+                              "phase_share": {n: float(mean[i] / mean[6]) for i, n in enumerate(names[:6])},
+                              "tuning": r.tuning()}), flush=True)
+        r.close()
+        index.close()
+        return
     gt = ground_truth(base, queries, k, w.metric, device, cache_dir) if rank == 0 else None
 
     d_q = torch.from_numpy(queries).to(device)
@@ -437,6 +475,7 @@ def main() -> None:
                        "recall_at_100": round(final_recall, 5), "parallelism": f"replicas{world}",
                        "l2": "256 MiB buffer written between timed steps (excluded from timing); "
                              "base vectors 512 MB > L2",
+                       "tuning": router.tuning(),
                        "graph_levels": report.get("vertices_by_highest_level"),
                        "graph_build_s": report.get("build_s")},
             "sweep": sweep,

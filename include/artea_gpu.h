@@ -140,6 +140,12 @@ typedef struct artea_gpu_router_opts {
     uint32_t max_batch;      /* largest nq one call may pass; 0 = 65536 */
     uint32_t max_queue;      /* largest per-query queue size; 0 = candidate_queue_size */
     uint32_t use_graphs;     /* capture launches in CUDA graphs and replay them */
+    uint32_t visited_hash_bits; /* log2 of the bucket count of the per-warp
+                                   shared-memory visited table (16 bytes per
+                                   bucket), in [6, 12]; 0 = autotuned;
+                                   0xFFFFFFFF = no table (HBM bitset only) */
+    uint32_t register_budget;   /* registers per thread of the persistent kernel:
+                                   64 or 85; 0 = autotuned */
 } artea_gpu_router_opts;
 
 /* Library / device information. */
@@ -202,6 +208,17 @@ int artea_gpu_router_sync(artea_gpu_router* router);
 
 /* Number of kernel launches this router has issued (for launch accounting). */
 int artea_gpu_router_launches(const artea_gpu_router* router, uint64_t* launches);
+
+/* Profiling hook: when d_phase_cycles (device memory, nq x 8 uint64) is set,
+ * every later launch writes per-query SM clock cycles spent in: greedy upper
+ * levels, pop/row lookup, row ids + visited, distances, queue merge, tail,
+ * total, and the count of expansions whose row lookup was prefetched. NULL
+ * turns it off. No reference counterpart (measurement only). */
+int artea_gpu_router_set_phase_buffer(artea_gpu_router* router, void* d_phase_cycles);
+
+/* Launch parameters of the router's last launch (the autotuner's choice). */
+int artea_gpu_router_tuning(const artea_gpu_router* router, uint32_t* warps_per_cta, uint32_t* visited_hash_bits,
+                            uint32_t* register_budget);
 
 #ifdef __cplusplus
 }

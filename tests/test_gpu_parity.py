@@ -191,3 +191,28 @@ def test_topk_larger_than_found_keeps_invalid_tail():
     ref = orc.batch_query(c.graph, c.base, c.queries, 4, 8, metric=1, k_stride=6)
     np.testing.assert_array_equal(out, ref)
     assert (entry_vids(out[:, 4:]) == 0x7FFFFFFF).all()
+
+
+@pytest.mark.parametrize("vh_bits,regs", [(6, 64), (6, 85), (10, 64), (10, 85)])
+def test_exact_with_visited_hash_spill_and_register_budgets(sift20k, vh_bits, regs):
+    # vh_bits=6 is a 64-bucket (512-slot) table, so every query here sends
+    # ids of full buckets to the HBM bitset; results must not change.
+    g, base, queries = sift20k
+    idx = DeviceIndex(g, base)
+    for warps in (2, 8):
+        r = GpuRouter(idx, 0, 100, 200, mode="exact", schedule="persistent", warps_per_cta=warps,
+                      visited_hash_bits=vh_bits, register_budget=regs)
+        out, st = r.batch_query(queries[:200], stats=True)
+        ref = orc.batch_query(g, base, queries[:200], 100, 200, metric=0)
+        np.testing.assert_array_equal(out, ref, err_msg=f"vh_bits={vh_bits} regs={regs} warps={warps}")
+        if vh_bits == 6:
+            assert (st[:, 7] > 0).all(), "expected every query to spill to the bitset"
+        assert r.tuning() == {"warps_per_cta": warps, "visited_hash_bits": vh_bits, "register_budget": regs}
+
+
+def test_plain_schedule_spill(sift20k):
+    g, base, queries = sift20k
+    idx = DeviceIndex(g, base)
+    r = GpuRouter(idx, 0, 100, 400, mode="exact", schedule="plain", visited_hash_bits=6)
+    out = r.batch_query(queries[:100])
+    np.testing.assert_array_equal(out, orc.batch_query(g, base, queries[:100], 100, 400, metric=0))
