@@ -280,6 +280,10 @@ int launch_with(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning
         a.vis_list = r->d_vis_list;
         CUDA_TRY(cudaMemsetAsync(r->d_counter, 0, sizeof(uint32_t), st));
         const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) * t.warps;
+        // The attribute is per kernel function and other launch shapes (other
+        // routers, autotuner candidates) change it: set it for every launch.
+        CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         fn<<<ctas, t.warps * 32, smem, st>>>(a);
     } else {
         if (int rc = ensure_slots(r, a.nq)) return rc;
@@ -694,3 +698,4 @@ int artea_gpu_router_launches(const artea_gpu_router* r, uint64_t* launches) {
 }
 
 }  // extern "C"
+

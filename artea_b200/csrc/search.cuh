@@ -489,6 +489,38 @@ __device__ __forceinline__ int queue_pop(Queue& q) {
     return p;
 }
 
+// pop_best_unexplored_entry, plus a peek at the entry that would come next if
+// nothing better is inserted meanwhile (-1 when none), in one scan.
+__device__ __forceinline__ int queue_pop_peek(Queue& q, int* next) {
+    const int lane = lane_id();
+    int first = -1;
+    *next = -1;
+    uint32_t base = q.hint;
+    for (; base < q.n; base += 32) {
+        const uint32_t idx = base + lane;
+        const bool un = idx < q.n && !(q.v[idx] & kExplored);
+        uint32_t b = __ballot_sync(kFull, un);
+        if (b) {
+            if (first < 0) {
+                first = static_cast<int>(base + __ffs(b) - 1);
+                b &= b - 1;
+            }
+            if (b) {
+                *next = static_cast<int>(base + __ffs(b) - 1);
+                break;
+            }
+        }
+    }
+    if (first < 0) {
+        q.hint = q.n;
+        return -1;
+    }
+    if (lane == 0) q.v[first] |= kExplored;
+    __syncwarp();
+    q.hint = static_cast<uint32_t>(first) + 1;
+    return first;
+}
+
 // try_push for a whole batch at once (std_candidate_queue.hpp:358-388).
 // Sequentially, candidate j is rejected iff T already holds L entries at
 // distance <= d_j. A rejected candidate never enters T, and every later
@@ -509,20 +541,24 @@ __device__ void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, uint32_
     uint32_t m = 0;
     for (uint32_t base = 0; base < cnt; base += 32) {
         const uint32_t j = base + lane;
+        const bool valid = j < cnt;
+        const float d = valid ? cdist[j] : INFINITY;
+        const uint32_t v = valid ? cvid[j] : 0u;
+        // pre = #{i < j : d_i <= d_j}: earlier chunks from shared memory, this
+        // chunk by shuffles.
+        uint32_t pre = 0;
+        for (uint32_t i = 0; i < base; ++i) pre += cdist[i] <= d ? 1u : 0u;
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k) {
+            const float dk = __shfl_sync(kFull, d, k);
+            pre += (k < lane && dk <= d) ? 1u : 0u;
+        }
+        // #{e in T : e.dist <= d} < L - pre  <=>  T[L-pre-1].dist > d (or T is
+        // shorter than L-pre).
         bool acc = false;
-        float d = 0.f;
-        uint32_t v = 0;
-        if (j < cnt) {
-            d = cdist[j];
-            v = cvid[j];
-            uint32_t lo = 0, hi = tn;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (q.d[mid] <= d) lo = mid + 1; else hi = mid;
-            }
-            uint32_t pre = 0;
-            for (uint32_t i = 0; i < j; ++i) pre += cdist[i] <= d ? 1u : 0u;
-            acc = lo + pre < q.L;
+        if (valid && pre < q.L) {
+            const uint32_t idx = q.L - pre - 1;
+            acc = idx >= tn || q.d[idx] > d;
         }
         const uint32_t b = __ballot_sync(kFull, acc);
         if (acc) {
@@ -809,7 +845,8 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
         bool pf_have_ids = false;
         for (uint32_t it = 0;; ++it) {
             if (it > g.n) { set_error(a.error, kErrBound); break; }
-            const int p = queue_pop(q);
+            int p2;
+            const int p = queue_pop_peek(q, &p2);
             if (p < 0) break;
             const uint32_t v = q.v[p] & kVidMask;
             if (v == kVidMask) break;   // CandidateEntry::is_invalid
@@ -826,7 +863,6 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                 ids0 = lane < len ? __ldg(row + lane) : 0xffffffffu;
                 ids1 = lane + 32 < len ? __ldg(row + lane + 32) : 0xffffffffu;
             }
-            const int p2 = queue_find_unexplored(q, q.hint);
             pf_have_ids = false;
             if (p2 >= 0) {
                 pf_vid = q.v[p2] & kVidMask;
