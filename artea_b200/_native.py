@@ -105,6 +105,8 @@ SIGNATURES = {
     "artea_gpu_router_sync": (c_int, [c_void_p]),
     "artea_gpu_router_launches": (c_int, [c_void_p, POINTER(c_uint64)]),
     "artea_gpu_router_set_phase_buffer": (c_int, [c_void_p, c_void_p]),
+    "artea_gpu_batch_query_noalloc": (c_int, [c_void_p, c_int, c_int, c_uint32, c_uint32, c_void_p, c_uint32, c_uint32,
+                                              c_void_p, c_void_p]),
     "artea_gpu_router_tuning": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32)]),
 }
 

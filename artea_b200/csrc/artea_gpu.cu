@@ -699,3 +699,164 @@ int artea_gpu_router_launches(const artea_gpu_router* r, uint64_t* launches) {
 
 }  // extern "C"
 
+// ===========================================================================
+// Batch query that allocates nothing.
+//
+// Some callers of this library cannot call cudaMalloc: code that runs inside
+// a framework's caching allocator or memory-pool callback (where a nested
+// allocation would re-enter the allocator), a serving thread that has
+// reserved every byte of device memory up front and treats any new
+// allocation as a fault, or a plugin whose host process forbids device
+// allocation after start-up. artea_gpu_batch_query_noalloc serves them: it
+// searches an already uploaded index with the persistent kernel, taking its
+// scratch memory (visited bitsets and lists, the work counter, the error
+// word) from g_noalloc_scratch, a fixed 64 MiB array that the CUDA loader
+// places on every device that loads this library and that stays there until
+// the process exits.
+//
+// Set-up: the first call on a device (with that device current) resolves the
+// array's device address with cudaGetSymbolAddress; make that first call
+// before any stream capture. All calls share the array and it keeps the last
+// call's contents, so each call zeroes the part it uses before the launch;
+// calls that overlap on the GPU (for example on two streams) race on it and
+// must be serialised by the caller. The call waits for its kernel so that it
+// can report kernel-side errors.
+// ===========================================================================
+namespace {
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;
+constexpr size_t kNoAllocHeader = 256;        // work counter + error word, padded
+constexpr uint32_t kNoAllocWarps = 4;
+constexpr uint32_t kNoAllocMaxQueue = 1024;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+struct NoAllocDevice {
+    bool ready = false;
+    unsigned char* scratch = nullptr;   // device address of g_noalloc_scratch
+    int num_sms = 0;
+};
+
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[64];
+
+int noalloc_device(int device, NoAllocDevice** out) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (device < 0 || device >= 64) return fail(ARTEA_GPU_EINVAL, "device index out of range");
+    NoAllocDevice& d = g_noalloc_dev[device];
+    if (!d.ready) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            return fail(ARTEA_GPU_ECUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
+                                             cudaGetErrorString(e));
+        }
+        int sms = 0;
+        CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        d.scratch = static_cast<unsigned char*>(p);
+        d.num_sms = sms;
+        d.ready = true;
+    }
+    *out = &d;
+    return ARTEA_GPU_OK;
+}
+
+}  // namespace
+
+extern "C" int artea_gpu_batch_query_noalloc(const artea_gpu_index* ix, int metric, int mode, uint32_t topk,
+                                             uint32_t queue_size, const float* d_queries, uint32_t nq,
+                                             uint32_t k_stride, uint64_t* d_out, void* stream) {
+    if (!ix) return fail(ARTEA_GPU_EINVAL, "null index");
+    if (metric < 0 || metric > 3) return fail(ARTEA_GPU_EINVAL, "unknown metric");
+    if (mode != ARTEA_GPU_MODE_EXACT && mode != ARTEA_GPU_MODE_FAST) return fail(ARTEA_GPU_EINVAL, "unknown mode");
+    if (queue_size < topk)
+        return fail(ARTEA_GPU_EINVAL, "candidate_queue_size (" + std::to_string(queue_size) + ") must be >= topk (" +
+                                          std::to_string(topk) + ")");
+    if (queue_size > kNoAllocMaxQueue)
+        return fail(ARTEA_GPU_EINVAL, "no-alloc query: queue size above the limit of " +
+                                          std::to_string(kNoAllocMaxQueue));
+    if (k_stride < topk) return fail(ARTEA_GPU_EINVAL, "k_stride must be >= topk");
+    if (nq == 0) return ARTEA_GPU_OK;
+    if (!d_queries || !d_out) return fail(ARTEA_GPU_EINVAL, "null query or output buffer");
+    if (reinterpret_cast<uintptr_t>(d_queries) % 16 != 0) return fail(ARTEA_GPU_EINVAL, "queries must be 16-byte aligned");
+    DeviceGuard guard(ix->device);
+    NoAllocDevice* dev = nullptr;
+    if (int rc = noalloc_device(ix->device, &dev)) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+    // Launch shape: 4 warps per CTA, the 85-register kernel, an 8 KB
+    // shared-memory visited table when the vid quotient fits in 15 bits.
+    const uint32_t cap = std::max<uint32_t>(2u * queue_size, 2u);
+    uint32_t kb = 1;
+    while (kb < 32 && (1ull << kb) < ix->n) ++kb;
+    uint32_t vh_bits = 9;
+    if (kb < vh_bits + 1) kb = vh_bits + 1;
+    if (kb - vh_bits >= 16) vh_bits = 0;
+    const uint32_t smem = smem_bytes_per_warp(ix->dim, cap, vh_bits) * kNoAllocWarps;
+    if (smem > 227u * 1024u) return fail(ARTEA_GPU_EINVAL, "no-alloc query: queue too large for shared memory");
+    KernelFn fn = pick_kernel(metric, mode == ARTEA_GPU_MODE_EXACT, true, 0);
+    CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(fn),
+                                                           static_cast<int>(kNoAllocWarps * 32), smem));
+    if (per_sm <= 0) return fail(ARTEA_GPU_EINVAL, "no-alloc query: kernel does not fit on an SM");
+
+    // Scratch layout: [counter, error | pad to 256] [bitsets: slots x words] [lists: slots x list_cap].
+    const uint64_t words = ((static_cast<uint64_t>(ix->n) + 127) / 128) * 4;
+    const uint32_t list_cap = std::max<uint32_t>(std::min<uint32_t>(ix->n, 4096), 64);
+    const uint64_t per_slot = words * 4 + static_cast<uint64_t>(list_cap) * 4;
+    const uint64_t max_slots = (kNoAllocScratchBytes - kNoAllocHeader) / per_slot;
+    uint64_t ctas = static_cast<uint64_t>(per_sm) * static_cast<uint64_t>(dev->num_sms);
+    ctas = std::min<uint64_t>(ctas, max_slots / kNoAllocWarps);
+    ctas = std::min<uint64_t>(ctas, (nq + kNoAllocWarps - 1) / kNoAllocWarps);
+    if (ctas == 0)
+        return fail(ARTEA_GPU_EINVAL, "no-alloc query: the graph needs " + std::to_string(per_slot * kNoAllocWarps) +
+                                          " bytes of scratch per CTA; the limit is 64 MiB");
+    const uint64_t slots = ctas * kNoAllocWarps;
+    unsigned char* base = dev->scratch;
+    uint32_t* d_counter = reinterpret_cast<uint32_t*>(base);
+    int* d_error = reinterpret_cast<int*>(base + 4);
+    uint32_t* bits = reinterpret_cast<uint32_t*>(base + kNoAllocHeader);
+    uint32_t* lists = bits + slots * words;
+    // The array keeps the previous call's contents: zero the counter, the
+    // error word and the bitsets this launch will use.
+    CUDA_TRY(cudaMemsetAsync(base, 0, kNoAllocHeader + slots * words * 4, st));
+
+    SearchArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g.vecs = ix->d_vecs;
+    a.g.vinfo = ix->d_vinfo;
+    a.g.nbrs = ix->d_nbrs;
+    a.g.l0row = ix->d_l0row;
+    a.g.n = ix->n;
+    a.g.dim = ix->dim;
+    a.g.top = ix->top;
+    a.g.entry = ix->entry;
+    for (int h = 0; h < kMaxGroups; ++h) a.g.offsets[h] = ix->group_ptr[h];
+    a.queries = d_queries;
+    a.nq = nq;
+    a.topk_default = topk;
+    a.queue_default = queue_size;
+    a.k_stride = k_stride;
+    a.cap = cap;
+    a.vh_bits = vh_bits;
+    a.vk_bits = kb;
+    a.out = d_out;
+    a.vis_bits = bits;
+    a.vis_list = lists;
+    a.words_per_slot = words;
+    a.list_cap = list_cap;
+    a.next_query = d_counter;
+    a.error = d_error;
+    fn<<<static_cast<unsigned>(ctas), kNoAllocWarps * 32, smem, st>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    int h_err = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h_err, d_error, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (h_err != 0) return fail(ARTEA_GPU_EKERNEL, "kernel error " + std::to_string(h_err) + " in no-alloc query");
+    return ARTEA_GPU_OK;
+}

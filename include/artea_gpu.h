@@ -220,6 +220,21 @@ int artea_gpu_router_set_phase_buffer(artea_gpu_router* router, void* d_phase_cy
 int artea_gpu_router_tuning(const artea_gpu_router* router, uint32_t* warps_per_cta, uint32_t* visited_hash_bits,
                             uint32_t* register_budget);
 
+/* batch_query on device buffers for callers that cannot allocate device
+ * memory (inside an allocator callback, under a fully reserved memory pool,
+ * or in a host process that forbids allocation after start-up). It allocates
+ * nothing: its scratch memory is a fixed 64 MiB array that every GPU loading
+ * this library holds until the process exits, so graphs whose per-CTA scratch
+ * (4 warps x (N/8 + 16 KiB) bytes) exceeds 64 MiB, and queues above 1024, are
+ * rejected with ARTEA_GPU_EINVAL. The first call on a device resolves the
+ * array's address (make it before any stream capture); calls share the array,
+ * so calls that overlap on the GPU race. Waits for its kernel before
+ * returning. No counterpart in the reference, whose router always allocates
+ * its visited tables and queues on the host. */
+int artea_gpu_batch_query_noalloc(const artea_gpu_index* index, int metric, int mode, uint32_t topk,
+                                  uint32_t queue_size, const float* d_queries, uint32_t nq, uint32_t k_stride,
+                                  uint64_t* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
