@@ -6,6 +6,9 @@
   (only where the reference headers are present; prebuilt copies travel).
 * ``oracle/`` — the test checkers (C restatement; reference router where the
   reference headers are present).
+* ``tests/cpp/_build/test_dropin`` — the C++ drop-in check (reference CPU
+  router vs artea::cuda::HierarchicalGraphRouter), where the reference
+  headers are present.
 
 Run ``python -m artea_b200.build`` or call ``build()``.
 """
@@ -73,6 +76,7 @@ def build(force: bool = False) -> None:
     build_make("oracle")
     if os.path.isdir(os.path.join(REF, "include")):
         build_make("index_build")
+        build_make(os.path.join("tests", "cpp"))
 
 
 if __name__ == "__main__":

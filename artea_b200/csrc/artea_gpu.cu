@@ -63,6 +63,19 @@ struct Tuning {
     uint32_t regs = 0;   // 0: 85-register budget, 1: 64-register budget
 };
 
+// Identity of a captured launch: the buffers, sizes and launch parameters.
+struct GraphKey {
+    const void* q;
+    const void* out;
+    const void* topk;
+    const void* queue;
+    const void* stats;
+    const void* phase;
+    uint32_t nq, k_stride, l0_only, pad;
+    uint64_t tuning;
+    bool operator<(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) < 0; }
+};
+
 struct artea_gpu_router {
     artea_gpu_index* idx = nullptr;
     uint32_t topk = 0, queue = 0, max_queue = 0, cap = 0, max_batch = 0;
@@ -95,6 +108,7 @@ struct artea_gpu_router {
     std::map<uint64_t, Tuning> tuned;           // (dim, queue capacity) -> launch parameters
     std::map<uint64_t, LaunchShape> shapes;     // (warps, hash bits) -> persistent grid
     Tuning last;                                // parameters of the last launch
+    std::map<GraphKey, cudaGraphExec_t> graphs; // captured launches (use_graphs)
 };
 
 namespace {
@@ -163,8 +177,19 @@ uint32_t smem_bytes_per_warp(uint32_t dim, uint32_t cap, uint32_t vh_bits) {
     return warp_smem_words(dim, cap, vh_bits) * 4u;
 }
 
+// Captured graphs hold buffer addresses: drop them whenever a buffer moves.
+void clear_graphs(artea_gpu_router* r) {
+    if (!r->graphs.empty()) {
+        cudaStreamSynchronize(r->stream);
+        cudaDeviceSynchronize();
+    }
+    for (auto& kv : r->graphs) cudaGraphExecDestroy(kv.second);
+    r->graphs.clear();
+}
+
 int ensure_slots(artea_gpu_router* r, uint32_t slots) {
     if (slots <= r->slots) return ARTEA_GPU_OK;
+    clear_graphs(r);
     dev_free(r->d_vis_bits);
     dev_free(r->d_vis_list);
     r->slots = 0;
@@ -178,6 +203,7 @@ int ensure_slots(artea_gpu_router* r, uint32_t slots) {
 
 int ensure_stage(artea_gpu_router* r, uint32_t nq, uint32_t k_stride) {
     if (nq <= r->stage_nq && k_stride <= r->stage_kstride) return ARTEA_GPU_OK;
+    clear_graphs(r);
     const uint32_t n2 = std::max(nq, r->stage_nq);
     const uint32_t k2 = std::max(k_stride, r->stage_kstride);
     dev_free(r->d_queries);
@@ -256,11 +282,22 @@ int fill_args(artea_gpu_router* r, SearchArgs* a, const float* d_q, uint32_t nq,
     return ARTEA_GPU_OK;
 }
 
-int launch_with(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning& t, cudaStream_t st) {
+// A launch made ready: kernel, grid, shared memory and final arguments. All
+// allocation (visited slots) and attribute setting happens here, so the
+// enqueue step can be captured into a CUDA graph.
+struct Prepared {
+    KernelFn fn = nullptr;
+    uint32_t grid = 0;
+    uint32_t threads = 0;
+    uint32_t smem = 0;
+    bool persistent = false;
+    SearchArgs a;
+};
+
+int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning& t, Prepared* p) {
     const bool exact = r->mode == ARTEA_GPU_MODE_EXACT;
     KernelFn fn = pick_kernel(r->metric, exact, persistent, t.regs);
     if (!fn) return fail(ARTEA_GPU_EINVAL, "unknown metric");
-    if (a.nq == 0) return ARTEA_GPU_OK;
     a.vh_bits = t.vh_bits;
     {
         uint32_t kb = 1;
@@ -270,33 +307,87 @@ int launch_with(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning
         // The 16-bit quotient (with 0xFFFF reserved) must hold kbits - tbits bits.
         if (a.vh_bits && kb - a.vh_bits >= 16) return fail(ARTEA_GPU_EINVAL, "visited table too small for N");
     }
+    p->fn = fn;
+    p->persistent = persistent;
     if (persistent) {
         LaunchShape s;
         if (int rc = persistent_shape(r, t, &s)) return rc;
         const uint32_t needed_ctas = (a.nq + t.warps - 1) / t.warps;
-        const uint32_t ctas = std::min(s.ctas, needed_ctas);
-        if (int rc = ensure_slots(r, ctas * t.warps)) return rc;
-        a.vis_bits = r->d_vis_bits;
-        a.vis_list = r->d_vis_list;
-        CUDA_TRY(cudaMemsetAsync(r->d_counter, 0, sizeof(uint32_t), st));
-        const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) * t.warps;
-        // The attribute is per kernel function and other launch shapes (other
-        // routers, autotuner candidates) change it: set it for every launch.
-        CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        fn<<<ctas, t.warps * 32, smem, st>>>(a);
+        p->grid = std::min(s.ctas, needed_ctas);
+        p->threads = t.warps * 32;
+        p->smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) * t.warps;
+        if (int rc = ensure_slots(r, p->grid * t.warps)) return rc;
     } else {
+        p->grid = a.nq;
+        p->threads = 32;
+        p->smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits);
         if (int rc = ensure_slots(r, a.nq)) return rc;
-        a.vis_bits = r->d_vis_bits;
-        a.vis_list = r->d_vis_list;
-        const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits);
-        CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        fn<<<a.nq, 32, smem, st>>>(a);
     }
+    a.vis_bits = r->d_vis_bits;
+    a.vis_list = r->d_vis_list;
+    // The attribute is per kernel function and other launch shapes (other
+    // routers, autotuner candidates) change it: set it for every launch.
+    CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(p->smem)));
+    p->a = a;
+    return ARTEA_GPU_OK;
+}
+
+int enqueue(artea_gpu_router* r, const Prepared& p, cudaStream_t st) {
+    if (p.persistent) CUDA_TRY(cudaMemsetAsync(r->d_counter, 0, sizeof(uint32_t), st));
+    p.fn<<<p.grid, p.threads, p.smem, st>>>(p.a);
+    CUDA_TRY(cudaGetLastError());
+    return ARTEA_GPU_OK;
+}
+
+int launch_with(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning& t, cudaStream_t st) {
+    if (a.nq == 0) return ARTEA_GPU_OK;
+    Prepared p;
+    if (int rc = prepare_launch(r, a, persistent, t, &p)) return rc;
+    if (int rc = enqueue(r, p, st)) return rc;
     r->last = t;
     r->launches++;
-    CUDA_TRY(cudaGetLastError());
+    return ARTEA_GPU_OK;
+}
+
+// CUDA-graph replay: the counter reset and the launch of one (buffers,
+// tuning) combination are captured once and replayed afterwards.
+int launch_graph(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning& t, cudaStream_t st) {
+    if (a.nq == 0) return ARTEA_GPU_OK;
+    Prepared p;
+    if (int rc = prepare_launch(r, a, persistent, t, &p)) return rc;
+    GraphKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.q = p.a.queries;
+    key.out = p.a.out;
+    key.topk = p.a.topk;
+    key.queue = p.a.queue;
+    key.stats = p.a.stats;
+    key.phase = p.a.phase_cycles;
+    key.nq = p.a.nq;
+    key.k_stride = p.a.k_stride;
+    key.l0_only = p.a.l0_only;
+    key.tuning = (static_cast<uint64_t>(t.warps) << 32) | (t.vh_bits << 1) | t.regs | (persistent ? 1ull << 63 : 0);
+    auto it = r->graphs.find(key);
+    if (it == r->graphs.end()) {
+        cudaGraph_t graph = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue(r, p, r->stream);
+        const cudaError_t ec = cudaStreamEndCapture(r->stream, &graph);
+        if (rc != ARTEA_GPU_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ec != cudaSuccess) return fail(ARTEA_GPU_ECUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) return fail(ARTEA_GPU_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        it = r->graphs.emplace(key, exec).first;
+    }
+    CUDA_TRY(cudaGraphLaunch(it->second, st));
+    r->last = t;
+    r->launches++;
     return ARTEA_GPU_OK;
 }
 
@@ -315,7 +406,7 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     auto it = r->tuned.find(key);
     if (it != r->tuned.end()) return it->second;
     static const uint32_t warp_choices[] = {2, 4, 8};
-    static const uint32_t bit_choices[] = {0, 9, 10, 11};
+    static const uint32_t bit_choices[] = {0, 8, 9, 10};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -390,6 +481,7 @@ int run_device(artea_gpu_router* r, const float* d_q, uint32_t nq, const uint32_
     t.warps = 1;
     t.vh_bits = r->want_vh_bits ? hash_bits_of(r->want_vh_bits) : 0;
     if (persistent) t = tuned(r, a, st);
+    if (r->use_graphs) return launch_graph(r, a, persistent, t, st);
     return launch_with(r, a, persistent, t, st);
 }
 
@@ -599,6 +691,7 @@ int artea_gpu_router_destroy(artea_gpu_router* r) {
     if (!r) return ARTEA_GPU_OK;
     DeviceGuard guard(r->idx->device);
     if (r->stream) cudaStreamSynchronize(r->stream);
+    clear_graphs(r);
     dev_free(r->d_vis_bits);
     dev_free(r->d_vis_list);
     dev_free(r->d_counter);

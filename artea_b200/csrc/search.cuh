@@ -159,20 +159,39 @@ __device__ float query_sqnorm(const float* __restrict__ q, uint32_t dim) {
 // before any arithmetic, so a D=128 row costs one memory round trip.
 constexpr int kBlock = 8;
 
+// Packed FP32x2 arithmetic (sm_100): each element is rounded on its own, as
+// two scalar instructions would round it, so the exact mode is unaffected;
+// the pair halves the instruction count of the accumulation.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ float lo32(f32x2 v) { return __uint_as_float(static_cast<uint32_t>(v)); }
+__device__ __forceinline__ float hi32(f32x2 v) { return __uint_as_float(static_cast<uint32_t>(v >> 32)); }
+
+// One chunk of 4 elements (x from the row, y from the query) into the pair
+// accumulators A01/A23 (and B01/B23 for cosine's x*x).
 template <int kMetric>
-__device__ __forceinline__ void accumulate(const float4 x, const float4 y, float& a0, float& a1, float& a2,
-                                           float& a3, float& b0, float& b1, float& b2, float& b3) {
+__device__ __forceinline__ void accumulate(const ulonglong2 x, const ulonglong2 y, f32x2& A01, f32x2& A23,
+                                           f32x2& B01, f32x2& B23) {
     if (kMetric == ARTEA_GPU_EUCLIDEAN_SQR || kMetric == ARTEA_GPU_EUCLIDEAN) {
-        const float d0 = __fsub_rn(y.x, x.x), d1 = __fsub_rn(y.y, x.y);
-        const float d2 = __fsub_rn(y.z, x.z), d3 = __fsub_rn(y.w, x.w);
-        a0 = fmaf(d0, d0, a0); a1 = fmaf(d1, d1, a1);
-        a2 = fmaf(d2, d2, a2); a3 = fmaf(d3, d3, a3);
+        const f32x2 d01 = sub2(y.x, x.x), d23 = sub2(y.y, x.y);
+        A01 = fma2(d01, d01, A01);
+        A23 = fma2(d23, d23, A23);
     } else {
-        a0 = fmaf(y.x, x.x, a0); a1 = fmaf(y.y, x.y, a1);
-        a2 = fmaf(y.z, x.z, a2); a3 = fmaf(y.w, x.w, a3);
+        A01 = fma2(y.x, x.x, A01);
+        A23 = fma2(y.y, x.y, A23);
         if (kMetric == ARTEA_GPU_COSINE) {
-            b0 = fmaf(x.x, x.x, b0); b1 = fmaf(x.y, x.y, b1);
-            b2 = fmaf(x.z, x.z, b2); b3 = fmaf(x.w, x.w, b3);
+            B01 = fma2(x.x, x.x, B01);
+            B23 = fma2(x.y, x.y, B23);
         }
     }
 }
@@ -200,22 +219,26 @@ __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ 
         const uint32_t vid = valid ? cvid[idx] : 0u;
         const float* row = g.vecs + static_cast<size_t>(vid) * dim + 4 * gi;
         const float* qq = q + 4 * gi;
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;   // L2: diff^2; dot/cos: q*x
-        float b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f;   // cos: x*x
+        f32x2 A01 = 0ull, A23 = 0ull;   // L2: diff^2; dot/cos: q*x   (+0.0f pairs)
+        f32x2 B01 = 0ull, B23 = 0ull;   // cos: x*x
         for (uint32_t cb = 0; cb < nchunks; cb += kBlock) {
-            float4 x[kBlock];
+            ulonglong2 x[kBlock];
 #pragma unroll
             for (int k = 0; k < kBlock; ++k) {
-                x[k] = (valid && cb + k < nchunks) ? ldg4(row + 16 * (cb + k)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                x[k] = (valid && cb + k < nchunks)
+                           ? __ldg(reinterpret_cast<const ulonglong2*>(row + 16 * (cb + k)))
+                           : make_ulonglong2(0ull, 0ull);
             }
 #pragma unroll
             for (int k = 0; k < kBlock; ++k) {
                 if (cb + k < nchunks) {
-                    const float4 y = *reinterpret_cast<const float4*>(qq + 16 * (cb + k));
-                    accumulate<kMetric>(x[k], y, a0, a1, a2, a3, b0, b1, b2, b3);
+                    const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(qq + 16 * (cb + k));
+                    accumulate<kMetric>(x[k], y, A01, A23, B01, B23);
                 }
             }
         }
+        const float a0 = lo32(A01), a1 = hi32(A01), a2 = lo32(A23), a3 = hi32(A23);
+        const float b0 = lo32(B01), b1 = hi32(B01), b2 = lo32(B23), b3 = hi32(B23);
         float res = fold16<kExact>(a0, a1, a2, a3);
         if (kMetric == ARTEA_GPU_EUCLIDEAN) {
             res = __fsqrt_rn(res);
@@ -538,25 +561,41 @@ __device__ void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, uint32_
     const int lane = lane_id();
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t tn = min(q.n, q.L);
+    // Only candidates closer than lb can enter a full T, and the earlier
+    // candidates a closer one must be counted against are closer as well:
+    // pre_j only involves "improving" candidates. Late in a search most
+    // batches have none.
+    const float lim = q.n >= q.L ? q.lb : INFINITY;
     uint32_t m = 0;
+    uint32_t improving_before = 0;   // improving candidates in earlier chunks
     for (uint32_t base = 0; base < cnt; base += 32) {
         const uint32_t j = base + lane;
         const bool valid = j < cnt;
         const float d = valid ? cdist[j] : INFINITY;
         const uint32_t v = valid ? cvid[j] : 0u;
+        const bool improving = valid && d < lim;
+        uint32_t imask = __ballot_sync(kFull, improving);
+        if (imask == 0 && improving_before == 0) continue;
         // pre = #{i < j : d_i <= d_j}: earlier chunks from shared memory, this
-        // chunk by shuffles.
+        // chunk by shuffles over the improving lanes only.
         uint32_t pre = 0;
-        for (uint32_t i = 0; i < base; ++i) pre += cdist[i] <= d ? 1u : 0u;
-#pragma unroll 8
-        for (int k = 0; k < 32; ++k) {
+        if (improving_before) {
+            for (uint32_t i = 0; i < base; ++i) pre += cdist[i] <= d ? 1u : 0u;
+        }
+        for (uint32_t bits = imask & lt_mask; __any_sync(kFull, bits != 0);) {
+            // each lane walks its own set of earlier improving lanes; shuffles
+            // need every lane, so lanes take turns through a uniform loop.
+            const int k = bits ? __ffs(bits) - 1 : 0;
             const float dk = __shfl_sync(kFull, d, k);
-            pre += (k < lane && dk <= d) ? 1u : 0u;
+            if (bits) {
+                pre += dk <= d ? 1u : 0u;
+                bits &= bits - 1;
+            }
         }
         // #{e in T : e.dist <= d} < L - pre  <=>  T[L-pre-1].dist > d (or T is
         // shorter than L-pre).
         bool acc = false;
-        if (valid && pre < q.L) {
+        if (improving && pre < q.L) {
             const uint32_t idx = q.L - pre - 1;
             acc = idx >= tn || q.d[idx] > d;
         }
@@ -567,6 +606,7 @@ __device__ void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, uint32_
             bv[k] = v;
         }
         m += __popc(b);
+        improving_before += __popc(imask);
     }
     __syncwarp();
     if (m == 0) return;

@@ -112,7 +112,8 @@ class GpuRouter:
 
     def __init__(self, index: DeviceIndex, metric, topk: int, candidate_queue_size: int, mode: str = "exact",
                  schedule: str = "auto", warps_per_cta: int = 0, ctas_per_sm: int = 0, max_batch: int = 0,
-                 max_queue: int = 0, visited_hash_bits: int = 0, register_budget: int = 0):
+                 max_queue: int = 0, visited_hash_bits: int = 0, register_budget: int = 0,
+                 use_graphs: bool = False):
         opts = nat.RouterOpts()
         opts.metric = metric_code(metric)
         opts.mode = MODES[mode] if isinstance(mode, str) else int(mode)
@@ -123,6 +124,7 @@ class GpuRouter:
         opts.max_queue = max_queue
         opts.visited_hash_bits = visited_hash_bits
         opts.register_budget = register_budget
+        opts.use_graphs = 1 if use_graphs else 0
         h = ctypes.c_void_p()
         nat.check(nat.lib().artea_gpu_router_create(index.handle, topk, candidate_queue_size, ctypes.byref(opts),
                                                     ctypes.byref(h)))

@@ -281,6 +281,7 @@ def main() -> None:
     ap.add_argument("--recall-target", type=float, default=0.95)
     ap.add_argument("--cpu-sample", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graphs", action="store_true", help="launch directly instead of replaying CUDA graphs")
     ap.add_argument("--reference-queue", type=int, default=0)
     ap.add_argument("--reference-sample", type=int, default=2000)
     ap.add_argument("--profile", action="store_true",
@@ -358,7 +359,8 @@ def main() -> None:
     stream = torch.cuda.current_stream(device)
 
     def make_router(L):
-        return GpuRouter(index, metric, k, L, mode=args.mode, schedule=args.schedule, max_batch=nq)
+        return GpuRouter(index, metric, k, L, mode=args.mode, schedule=args.schedule, max_batch=nq,
+                         use_graphs=not args.no_graphs)
 
     # Queue sweep: recall per queue size (rank 0 decides, all ranks follow).
     queues = [int(x) for x in args.queues.split(",") if x]
@@ -472,6 +474,7 @@ def main() -> None:
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": w.name, "n_base": w.n_base, "n_query": nq, "dim": dim, "metric": w.metric,
                        "topk": k, "queue": chosen, "mode": args.mode, "schedule": args.schedule,
+                       "cuda_graphs": not args.no_graphs,
                        "recall_at_100": round(final_recall, 5), "parallelism": f"replicas{world}",
                        "l2": "256 MiB buffer written between timed steps (excluded from timing); "
                              "base vectors 512 MB > L2",

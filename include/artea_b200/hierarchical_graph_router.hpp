@@ -1,0 +1,214 @@
+// artea::cuda::HierarchicalGraphRouter — drop-in for the reference router.
+//
+// Same template and call surface as the CPU router
+// (include/artea/cpu/router/hierarchical_graph_router.hpp:66-430, reached as
+// hierarchical_graph_router_t<Metric, Dim>, framework/type_context/default_context.hpp:158):
+//
+//   artea::cuda::HierarchicalGraphRouter<router_traits_t<Metric, Dim>> r(base_vecs, dist, topk, queue);
+//   r.initialize();
+//   knn_results_t res = r.batch_query</*RandomSeeding=*/false>(query_vecs, compact_hg);
+//
+// Header-only; it depends on the reference only through the traits and graph
+// types it is instantiated with, and on libartea_gpu.so through the C-ABI of
+// include/artea_gpu.h. The first batch_query with a graph uploads the graph and
+// base_vecs (the router keeps a const reference to base_vecs, as the reference
+// does, router/vector_router.hpp:46,63-69) and later calls reuse the device
+// copy, keyed by the graph's address. Errors surface as std::runtime_error
+// (the reference's ARTEA_ERROR, common/logger.hpp:97-99,149).
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../artea_gpu.h"
+
+namespace artea {
+namespace cuda {
+
+namespace detail {
+
+inline void check(int status, const char* what) {
+    if (status != ARTEA_GPU_OK) {
+        throw std::runtime_error(std::string(what) + ": " + artea_gpu_last_error());
+    }
+}
+
+// DistanceMetricsT of the traits -> artea_gpu_metric (simd_distance.hpp:64-79).
+template <typename RouterTraitsT>
+constexpr int metric_code() {
+    using M = typename RouterTraitsT::distance_metrics_t;
+    constexpr M m = RouterTraitsT::distance_metrics;
+    if constexpr (m == M::EUCLIDEAN_SQR) return ARTEA_GPU_EUCLIDEAN_SQR;
+    else if constexpr (m == M::EUCLIDEAN) return ARTEA_GPU_EUCLIDEAN;
+    else if constexpr (m == M::COSINE) return ARTEA_GPU_COSINE;
+    else return ARTEA_GPU_DOT;
+}
+
+}  // namespace detail
+
+/** Options beyond the reference's ctor: distance mode (EXACT reproduces the
+ *  reference bit for bit), schedule and device. */
+struct RouterOptions {
+    int mode = ARTEA_GPU_MODE_EXACT;
+    int schedule = ARTEA_GPU_SCHEDULE_AUTO;
+    int device = 0;
+};
+
+template <typename RouterTraitsT>
+class HierarchicalGraphRouter {
+public:
+    using vertex_num_t = typename RouterTraitsT::vertex_num_t;
+    using vertex_id_t = typename RouterTraitsT::vertex_id_t;
+    using vec_ele_t = typename RouterTraitsT::vec_ele_t;
+    using dist_func_t = typename RouterTraitsT::dist_func_t;
+    using vector_array_t = typename RouterTraitsT::vector_array_t;
+    using query_vecs_t = typename RouterTraitsT::query_vecs_t;
+    using candidate_entry_t = typename RouterTraitsT::candidate_entry_t;
+    using knn_results_t = typename RouterTraitsT::knn_results_t;
+
+    static_assert(sizeof(candidate_entry_t) == 8, "results are 8-byte CandidateEntry words");
+    static_assert(std::is_same_v<vec_ele_t, float>, "the GPU router searches FP32 vectors");
+    static_assert(RouterTraitsT::vec_dim % 16 == 0, "Dim must be the SIMD-padded dimension (multiple of 16)");
+
+    HierarchicalGraphRouter(const vector_array_t& base_vecs, const dist_func_t& dist_func, const uint32_t topk,
+                            const vertex_num_t candidate_queue_size = 16, RouterOptions opts = {})
+        : _vecs(base_vecs), _dist(dist_func), _topk(topk), _queue(candidate_queue_size), _opts(opts),
+          _state(std::make_shared<State>()) {
+        // hierarchical_graph_router.hpp:104-108
+        if (candidate_queue_size < topk) {
+            throw std::runtime_error("candidate_queue_size (" + std::to_string(candidate_queue_size) +
+                                     ") must be >= topk (" + std::to_string(topk) + ")");
+        }
+    }
+
+    /** hierarchical_graph_router.hpp:114-117. Checks that a device is usable;
+     *  device state is created per graph on first use. */
+    auto initialize() -> void {
+        int n = 0;
+        detail::check(artea_gpu_device_count(&n), "artea_gpu_device_count");
+        if (_opts.device >= n) throw std::runtime_error("CUDA device not available");
+    }
+
+    /** batch_query<RandomSeeding, enable_early_stop>(query_vecs, graph)
+     *  (hierarchical_graph_router.hpp:293-349): nq*topk entries, row-major,
+     *  invalid-filled past each query's results. */
+    template <bool RandomSeeding = false, bool enable_early_stop = false, typename HierarchicalGraphT>
+    auto batch_query(const query_vecs_t& query_vecs, const HierarchicalGraphT& hier_graph) const -> knn_results_t {
+        static_assert(!RandomSeeding, "the GPU router seeds from the graph's entry point (RandomSeeding=false)");
+        static_assert(!enable_early_stop, "upper-level early stopping is not offered by the GPU router");
+        static_assert(HierarchicalGraphT::is_compacted, "the GPU router searches compact graphs");
+        return _run(query_vecs.get_all(), query_vecs.get_num_vecs(), hier_graph, false);
+    }
+
+    /** query(query_vec, graph): at most topk entries (hierarchical_graph_router.hpp:164-174). */
+    template <bool RandomSeeding = false, bool enable_early_stop = false, typename HierarchicalGraphT>
+    auto query(const vec_ele_t* query_vec, const HierarchicalGraphT& hier_graph) const -> knn_results_t {
+        static_assert(!RandomSeeding && !enable_early_stop, "see batch_query");
+        auto res = _run(query_vec, 1, hier_graph, false);
+        while (!res.empty() && res.back().is_invalid()) res.pop_back();
+        return res;
+    }
+
+    /** batch_query_l0_only (hierarchical_graph_router.hpp:353-385). */
+    template <bool RandomSeeding = false, typename HierarchicalGraphT>
+    auto batch_query_l0_only(const query_vecs_t& query_vecs, const HierarchicalGraphT& hier_graph) const
+        -> knn_results_t {
+        static_assert(!RandomSeeding, "see batch_query");
+        static_assert(HierarchicalGraphT::is_compacted, "batch_query_l0_only is only defined for compact graphs.");
+        return _run(query_vecs.get_all(), query_vecs.get_num_vecs(), hier_graph, true);
+    }
+
+private:
+    struct Device {
+        artea_gpu_index* index = nullptr;
+        artea_gpu_router* router = nullptr;
+        ~Device() {
+            if (router) artea_gpu_router_destroy(router);
+            if (index) artea_gpu_index_destroy(index);
+        }
+    };
+    struct State {
+        std::mutex mu;
+        std::map<const void*, std::unique_ptr<Device>> by_graph;
+    };
+
+    template <typename HierarchicalGraphT>
+    auto _device_for(const HierarchicalGraphT& g) const -> Device& {
+        std::lock_guard<std::mutex> lk(_state->mu);
+        auto it = _state->by_graph.find(&g);
+        if (it != _state->by_graph.end()) return *it->second;
+        // compact::HierarchicalGraph -> artea_gpu_graph_desc
+        // (compact_structure/hierarchical_graph.hpp:46-49, 83-121).
+        const uint32_t n = g.get_num_vertices();
+        const uint32_t top = g.top_occupied_level_id();
+        const bool empty = top == HierarchicalGraphT::invalid_level_id;
+        std::vector<const uint64_t*> offsets;
+        std::vector<uint64_t> sizes;
+        if (!empty) {
+            for (uint32_t h = 0; h <= top; ++h) {
+                offsets.push_back(g.get_nbr_offsets(h).data());
+                sizes.push_back(g.get_vids_with_highest_level(h).size());
+            }
+        } else {
+            sizes.push_back(0);
+        }
+        static_assert(sizeof(typename HierarchicalGraphT::VertexInfo) == 8, "vertex table of {level, local id}");
+        artea_gpu_graph_desc d{};
+        d.num_vertices = n;
+        d.top_level = empty ? 0xFFFFFFFFu : top;
+        d.ul_max_nbr_size = g.ul_max_nbr_size();
+        d.bl_max_nbr_size = g.bl_max_nbr_size();
+        d.entry_point_vid = g.entry_point_vid();
+        d.vertex_info = n ? reinterpret_cast<const uint32_t*>(&g.get_vertex_info(0)) : nullptr;
+        d.group_offsets = offsets.data();
+        d.group_sizes = sizes.data();
+        d.neighbor_ids = g.neighbor_ids().data();
+        d.num_neighbor_ids = g.neighbor_ids().size();
+        auto dev = std::make_unique<Device>();
+        detail::check(artea_gpu_index_create(&d, _vecs.get_all(), _vecs.get_num_vecs(), _vecs.get_vec_dim(),
+                                             _opts.device, &dev->index),
+                      "artea_gpu_index_create");
+        artea_gpu_router_opts o{};
+        o.metric = detail::metric_code<RouterTraitsT>();
+        o.mode = _opts.mode;
+        o.schedule = _opts.schedule;
+        detail::check(artea_gpu_router_create(dev->index, _topk, _queue, &o, &dev->router), "artea_gpu_router_create");
+        auto& ref = *dev;
+        _state->by_graph.emplace(&g, std::move(dev));
+        return ref;
+    }
+
+    template <typename HierarchicalGraphT>
+    auto _run(const vec_ele_t* queries, uint32_t nq, const HierarchicalGraphT& g, bool l0_only) const
+        -> knn_results_t {
+        Device& dev = _device_for(g);
+        knn_results_t results(static_cast<std::size_t>(nq) * _topk, candidate_entry_t::make_invalid_entry());
+        if (nq == 0 || _topk == 0) return results;
+        std::vector<uint64_t> words(static_cast<std::size_t>(nq) * _topk);
+        const int rc = l0_only
+                           ? artea_gpu_batch_query_l0_only(dev.router, queries, nq, _topk, words.data(), nullptr)
+                           : artea_gpu_batch_query(dev.router, queries, nq, nullptr, nullptr, _topk, words.data(),
+                                                   nullptr);
+        detail::check(rc, "artea_gpu_batch_query");
+        std::memcpy(static_cast<void*>(results.data()), words.data(), words.size() * sizeof(uint64_t));
+        return results;
+    }
+
+    const vector_array_t& _vecs;
+    const dist_func_t& _dist;
+    uint32_t _topk;
+    vertex_num_t _queue;
+    RouterOptions _opts;
+    std::shared_ptr<State> _state;
+};
+
+}  // namespace cuda
+}  // namespace artea
