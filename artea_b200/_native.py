@@ -15,9 +15,9 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libartea_gpu.so")
 HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "artea_gpu.h")
 
-OK, EINVAL, ENOMEM, ECUDA, EGRAPH, EIO, EKERNEL, ETIMEOUT, ENODEV = range(9)
+OK, EINVAL, ENOMEM, ECUDA, EGRAPH, EIO, EKERNEL, ETIMEOUT, ENODEV, EBUSY = range(10)
 STATUS_NAMES = {OK: "OK", EINVAL: "EINVAL", ENOMEM: "ENOMEM", ECUDA: "ECUDA", EGRAPH: "EGRAPH", EIO: "EIO",
-                EKERNEL: "EKERNEL", ETIMEOUT: "ETIMEOUT", ENODEV: "ENODEV"}
+                EKERNEL: "EKERNEL", ETIMEOUT: "ETIMEOUT", ENODEV: "ENODEV", EBUSY: "EBUSY"}
 
 METRIC_EUCLIDEAN_SQR, METRIC_EUCLIDEAN, METRIC_COSINE, METRIC_DOT = 0, 1, 2, 3
 MODE_EXACT, MODE_FAST = 0, 1
@@ -81,6 +81,18 @@ class RouterOpts(ctypes.Structure):
     ]
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [
+        ("metric", c_int),
+        ("mode", c_int),
+        ("max_topk", c_uint32),
+        ("max_queue", c_uint32),
+        ("ring_slots", c_uint32),
+        ("warps_per_cta", c_uint32),
+        ("idle_polls", c_uint32),
+    ]
+
+
 # Every exported function with its ctypes signature; the names are exactly
 # the functions include/artea_gpu.h declares.
 SIGNATURES = {
@@ -105,6 +117,11 @@ SIGNATURES = {
     "artea_gpu_router_sync": (c_int, [c_void_p]),
     "artea_gpu_router_launches": (c_int, [c_void_p, POINTER(c_uint64)]),
     "artea_gpu_router_set_phase_buffer": (c_int, [c_void_p, c_void_p]),
+    "artea_gpu_server_create": (c_int, [c_void_p, POINTER(ServerOpts), POINTER(c_void_p)]),
+    "artea_gpu_server_submit": (c_int, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, POINTER(c_uint64)]),
+    "artea_gpu_server_poll": (c_int, [c_void_p, c_uint64, c_uint32, c_uint32, c_void_p, POINTER(c_int)]),
+    "artea_gpu_server_stats": (c_int, [c_void_p, POINTER(c_uint64), POINTER(c_uint64), POINTER(c_uint64)]),
+    "artea_gpu_server_destroy": (c_int, [c_void_p]),
     "artea_gpu_batch_query_noalloc": (c_int, [c_void_p, c_int, c_int, c_uint32, c_uint32, c_void_p, c_uint32, c_uint32,
                                               c_void_p, c_void_p]),
     "artea_gpu_router_tuning": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32)]),

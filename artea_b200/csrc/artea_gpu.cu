@@ -14,6 +14,7 @@
 
 #include "../../include/artea_gpu.h"
 #include "common.h"
+#include "internal.h"
 #include "search.cuh"
 
 namespace artea_gpu {
@@ -28,26 +29,6 @@ int fail(int code, const std::string& msg) {
 }
 
 }  // namespace artea_gpu
-
-using artea_gpu::fail;
-
-#define CUDA_TRY(expr)                                                                              \
-    do {                                                                                            \
-        cudaError_t _e = (expr);                                                                    \
-        if (_e != cudaSuccess) return fail(ARTEA_GPU_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
-    } while (0)
-
-struct artea_gpu_index {
-    int device = 0;
-    uint32_t n = 0, dim = 0, top = artea_gpu::kInvalidLevel, entry = 0, ul = 0, bl = 0;
-    float* d_vecs = nullptr;
-    uint2* d_vinfo = nullptr;
-    uint32_t* d_nbrs = nullptr;
-    uint64_t* d_offsets = nullptr;
-    unsigned long long* d_l0row = nullptr;
-    const uint64_t* group_ptr[artea_gpu::kMaxGroups] = {};
-    uint64_t bytes = 0;
-};
 
 struct LaunchShape {
     uint32_t warps_per_cta = 0;
@@ -118,37 +99,6 @@ using namespace artea_gpu;
 // Router option visited_hash_bits: 0 = autotuned, ~0u = no hash, else log2 size.
 constexpr uint32_t kNoHash = 0xffffffffu;
 uint32_t hash_bits_of(uint32_t want) { return want == kNoHash ? 0u : want; }
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
-
-template <typename T>
-int dev_alloc(T** p, size_t count) {
-    *p = nullptr;
-    if (count == 0) return ARTEA_GPU_OK;
-    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * count);
-    if (e != cudaSuccess) {
-        *p = nullptr;
-        cudaGetLastError();
-        return fail(e == cudaErrorMemoryAllocation ? ARTEA_GPU_ENOMEM : ARTEA_GPU_ECUDA,
-                    std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    }
-    return ARTEA_GPU_OK;
-}
-
-template <typename T>
-void dev_free(T*& p) {
-    if (p) cudaFree(p);
-    p = nullptr;
-}
 
 using KernelFn = void (*)(SearchArgs);
 

@@ -1,0 +1,69 @@
+// Host-side internals shared by the C-ABI translation units: the index
+// structure, error macro, device guard and device allocation helpers.
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/artea_gpu.h"
+#include "common.h"
+#include "search.cuh"
+
+using artea_gpu::fail;
+
+#define CUDA_TRY(expr)                                                                              \
+    do {                                                                                            \
+        cudaError_t _e = (expr);                                                                    \
+        if (_e != cudaSuccess) return fail(ARTEA_GPU_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+// A device-resident graph plus its vectors (artea_gpu_index_create).
+struct artea_gpu_index {
+    int device = 0;
+    uint32_t n = 0, dim = 0, top = artea_gpu::kInvalidLevel, entry = 0, ul = 0, bl = 0;
+    float* d_vecs = nullptr;
+    uint2* d_vinfo = nullptr;
+    uint32_t* d_nbrs = nullptr;
+    uint64_t* d_offsets = nullptr;
+    unsigned long long* d_l0row = nullptr;
+    const uint64_t* group_ptr[artea_gpu::kMaxGroups] = {};
+    uint64_t bytes = 0;
+};
+
+namespace artea_gpu {
+
+// Makes a device current for a scope.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+template <typename T>
+inline int dev_alloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) return ARTEA_GPU_OK;
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * count);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? ARTEA_GPU_ENOMEM : ARTEA_GPU_ECUDA,
+                    std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return ARTEA_GPU_OK;
+}
+
+template <typename T>
+inline void dev_free(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+}  // namespace artea_gpu

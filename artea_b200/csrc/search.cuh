@@ -80,6 +80,7 @@ struct SearchArgs {
     int* __restrict__ error;
     uint32_t l0_only;
     unsigned long long* __restrict__ phase_cycles;   // nq x kPhases, optional
+    uint32_t coherent;        // queries/topk/queue may change while the kernel runs (serving ring)
 };
 
 // Phase-cycle breakdown written per query when phase_cycles is set.
@@ -359,7 +360,7 @@ __device__ __forceinline__ void table_reset(const Visited& vs) {
     }
 }
 
-__device__ void visited_clear(Visited& vs) {
+__device__ inline void visited_clear(Visited& vs) {
     const int lane = lane_id();
     __syncwarp();
     table_reset(vs);
@@ -556,7 +557,7 @@ __device__ __forceinline__ int queue_pop_peek(Queue& q, int* next) {
 // in between are worse than every later lb).
 // Scratch: bd/bv hold the accepted batch; cdist/cvid are reused for its
 // sorted copy.
-__device__ void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, uint32_t cnt, float* bd, uint32_t* bv,
+__device__ inline void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, uint32_t cnt, float* bd, uint32_t* bv,
                                  int* error) {
     const int lane = lane_id();
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -768,8 +769,8 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
     const int lane = lane_id();
     const DeviceGraph& g = a.g;
     const uint32_t dim = g.dim;
-    const uint32_t topk = a.topk ? a.topk[qi] : a.topk_default;
-    const uint32_t L = a.queue ? a.queue[qi] : a.queue_default;
+    const uint32_t topk = a.topk ? (a.coherent ? __ldcg(a.topk + qi) : a.topk[qi]) : a.topk_default;
+    const uint32_t L = a.queue ? (a.coherent ? __ldcg(a.queue + qi) : a.queue[qi]) : a.queue_default;
     uint64_t* out = a.out + static_cast<size_t>(qi) * a.k_stride;
     constexpr uint64_t kInvalidWord = (static_cast<uint64_t>(0x7f7fffffu) << 32) | kVidMask;
 
@@ -804,7 +805,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
         // Stage the query row in shared memory; reset the visited hash.
         const float4* src = reinterpret_cast<const float4*>(a.queries + static_cast<size_t>(qi) * dim);
         float4* dst = reinterpret_cast<float4*>(sm.q);
-        for (uint32_t i = lane; i < dim / 4; i += 32) dst[i] = __ldg(src + i);
+        for (uint32_t i = lane; i < dim / 4; i += 32) dst[i] = a.coherent ? __ldcg(src + i) : __ldg(src + i);
         table_reset(vs);
         __syncwarp();
         const float qsq = (kMetric == ARTEA_GPU_COSINE) ? query_sqnorm<kExact>(sm.q, dim) : 0.f;

@@ -53,7 +53,8 @@ typedef enum artea_gpu_status {
     ARTEA_GPU_EIO = 5,       /* snapshot file missing, truncated or malformed */
     ARTEA_GPU_EKERNEL = 6,   /* a kernel reported an internal error (bound exceeded) */
     ARTEA_GPU_ETIMEOUT = 7,  /* a bounded wait gave up */
-    ARTEA_GPU_ENODEV = 8     /* no usable CUDA device */
+    ARTEA_GPU_ENODEV = 8,    /* no usable CUDA device */
+    ARTEA_GPU_EBUSY = 9      /* serving ring full: poll finished requests first */
 } artea_gpu_status;
 
 /* DistanceMetricsT values the router is instantiated with
@@ -219,6 +220,42 @@ int artea_gpu_router_set_phase_buffer(artea_gpu_router* router, void* d_phase_cy
 /* Launch parameters of the router's last launch (the autotuner's choice). */
 int artea_gpu_router_tuning(const artea_gpu_router* router, uint32_t* warps_per_cta, uint32_t* visited_hash_bits,
                             uint32_t* register_budget);
+
+/* ---- Serving loop (continuous batching) ----
+ * No counterpart in the reference, whose batch_query is one blocking call; each
+ * query gets the reference's _query (hierarchical_graph_router.hpp:195-248).
+ * A server keeps the index, a ring of per-query slots (query row, topk, queue,
+ * result row) and one persistent kernel on the device. submit() admits a
+ * request of n queries when n ring slots are free (else ARTEA_GPU_EBUSY),
+ * copies it in and publishes it to the running kernel, which claims queries
+ * one per warp; queries of requests submitted while others run overlap on the
+ * device. poll() reports a request done once all its queries are; it copies
+ * their rows out and frees the slots. The kernel exits after idle_polls idle
+ * polls (about 1 us each); submit()/poll() relaunch it when work is pending. */
+typedef struct artea_gpu_server artea_gpu_server;
+
+typedef struct artea_gpu_server_opts {
+    int metric;              /* artea_gpu_metric */
+    int mode;                /* artea_gpu_mode */
+    uint32_t max_topk;       /* largest topk of any query (result row width) */
+    uint32_t max_queue;      /* largest queue size of any query */
+    uint32_t ring_slots;     /* queries in flight (admission limit) */
+    uint32_t warps_per_cta;  /* 0 = 2 */
+    uint32_t idle_polls;     /* 0 = 5000 */
+} artea_gpu_server_opts;
+
+int artea_gpu_server_create(artea_gpu_index* index, const artea_gpu_server_opts* opts, artea_gpu_server** out);
+/* queries: n x dim host FP32; topk/queue: n per-query values or NULL (the maxima).
+ * *ticket identifies the request for poll(). */
+int artea_gpu_server_submit(artea_gpu_server* server, const float* queries, uint32_t n, const uint32_t* topk,
+                            const uint32_t* queue, uint64_t* ticket);
+/* *done = 1 and out_entries (n x k_stride words) filled once every query of the
+ * request finished; *done = 0 otherwise. */
+int artea_gpu_server_poll(artea_gpu_server* server, uint64_t ticket, uint32_t n, uint32_t k_stride,
+                          uint64_t* out_entries, int* done);
+int artea_gpu_server_stats(const artea_gpu_server* server, uint64_t* published, uint64_t* consumed,
+                           uint64_t* kernel_launches);
+int artea_gpu_server_destroy(artea_gpu_server* server);
 
 /* batch_query on device buffers for callers that cannot allocate device
  * memory (inside an allocator callback, under a fully reserved memory pool,
