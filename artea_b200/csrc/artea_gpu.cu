@@ -2,6 +2,8 @@
 // The kernels live in search.cuh; this file owns memory, streams, launch
 // configuration, the autotuner and the host-buffer entry points.
 #include <algorithm>
+#include <cfloat>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -90,6 +92,8 @@ struct artea_gpu_router {
     std::map<uint64_t, LaunchShape> shapes;     // (warps, hash bits) -> persistent grid
     Tuning last;                                // parameters of the last launch
     std::map<GraphKey, cudaGraphExec_t> graphs; // captured launches (use_graphs)
+    bool early_stop = false;                    // artea_gpu_router_set_early_stop
+    float es_thr[artea_gpu::kMaxGroups] = {};
 };
 
 namespace {
@@ -229,6 +233,8 @@ int fill_args(artea_gpu_router* r, SearchArgs* a, const float* d_q, uint32_t nq,
     a->error = r->d_error;
     a->l0_only = l0_only ? 1u : 0u;
     a->phase_cycles = r->d_phase;
+    a->early_stop = r->early_stop ? 1u : 0u;
+    for (int h = 0; h < kMaxGroups; ++h) a->es_thr[h] = r->es_thr[h];
     return ARTEA_GPU_OK;
 }
 
@@ -722,6 +728,32 @@ int artea_gpu_router_sync(artea_gpu_router* r) {
 int artea_gpu_router_set_phase_buffer(artea_gpu_router* r, void* d_phase_cycles) {
     if (!r) return fail(ARTEA_GPU_EINVAL, "null router");
     r->d_phase = static_cast<unsigned long long*>(d_phase_cycles);
+    return ARTEA_GPU_OK;
+}
+
+// _early_stop_thresholds (hierarchical_graph_router.hpp:388-408): per level
+// h in [1, top], the configuration's threshold in double, squared for
+// EUCLIDEAN_SQR, must stay a positive finite float that does not round to 0.
+int artea_gpu_router_set_early_stop(artea_gpu_router* r, const float* level_thresholds, uint32_t n_levels) {
+    if (!r) return fail(ARTEA_GPU_EINVAL, "null router");
+    float thr[kMaxGroups] = {};
+    const bool on = level_thresholds != nullptr && n_levels != 0;
+    const uint32_t top = r->idx->top;
+    if (on && top != kInvalidLevel && top != 0) {
+        if (n_levels <= top)
+            return fail(ARTEA_GPU_EINVAL, "early-stop thresholds cover levels [0, " + std::to_string(n_levels) +
+                                              ") but the graph's top level is " + std::to_string(top));
+        for (uint32_t h = 1; h <= top; ++h) {
+            double t = static_cast<double>(level_thresholds[h]);
+            if (r->metric == ARTEA_GPU_EUCLIDEAN_SQR) t *= t;
+            if (!std::isfinite(t) || t <= 0.0 || t > static_cast<double>(FLT_MAX) || static_cast<float>(t) == 0.0f)
+                return fail(ARTEA_GPU_EINVAL, "Early-stop threshold is not representable in query distance units");
+            thr[h] = static_cast<float>(t);
+        }
+    }
+    clear_graphs(r);   // captured launches hold the old arguments
+    r->early_stop = on;
+    std::memcpy(r->es_thr, thr, sizeof(thr));
     return ARTEA_GPU_OK;
 }
 

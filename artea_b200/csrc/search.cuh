@@ -1,7 +1,7 @@
 // Device side of the B200 query path: one warp searches one query.
 //
 // Restates, on the GPU, hierarchical_graph_router.hpp:195-248 (_query with
-// RandomSeeding=false, enable_early_stop=false): entry point, greedy descent
+// RandomSeeding=false; enable_early_stop either way): entry point, greedy descent
 // on levels top..1 (detail/beam_loop.hpp:129-166), beam search on level 0
 // (detail/beam_loop.hpp:90-119) with StdCandidateQueue's rules
 // (router/data_structures/std_candidate_queue.hpp:358-513), top-k extraction
@@ -81,6 +81,8 @@ struct SearchArgs {
     uint32_t l0_only;
     unsigned long long* __restrict__ phase_cycles;   // nq x kPhases, optional
     uint32_t coherent;        // queries/topk/queue may change while the kernel runs (serving ring)
+    uint32_t early_stop;      // stop level-h greedy walks at distance <= es_thr[h]
+    float es_thr[kMaxGroups]; // per-level thresholds in query distance units
 };
 
 // Phase-cycle breakdown written per query when phase_cycles is set.
@@ -824,6 +826,8 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                 visited_set(vs, cur);
                 for (uint32_t hop = 0;; ++hop) {
                     if (hop > g.n) { set_error(a.error, kErrBound); break; }
+                    // enable_early_stop: detail/beam_loop.hpp:147-150.
+                    if (a.early_stop && cur_d <= a.es_thr[h]) break;
                     uint32_t len;
                     const uint32_t* row = level_row(g, cur, h, &len);
                     ct.upper_rows++;

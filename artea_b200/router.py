@@ -20,7 +20,7 @@ from typing import Optional
 import numpy as np
 
 from . import _native as nat
-from .graph import CompactHierarchicalGraph
+from .graph import INVALID_LEVEL, CompactHierarchicalGraph
 
 METRICS = {
     "euclidean_sqr": nat.METRIC_EUCLIDEAN_SQR,
@@ -174,6 +174,22 @@ class GpuRouter:
     def sync(self) -> None:
         nat.check(nat.lib().artea_gpu_router_sync(self._h))
 
+    def set_early_stop(self, level_thresholds) -> None:
+        """enable_early_stop=true for later launches: level_thresholds[h] is the
+        configuration's early_stop_threshold(h, pruning) (index 0 unused); None
+        switches it off. OverflowError when a threshold is not representable in
+        query units (hierarchical_graph_router.hpp:398-404)."""
+        if level_thresholds is None:
+            nat.check(nat.lib().artea_gpu_router_set_early_stop(self._h, None, 0))
+            return
+        thr = np.ascontiguousarray(level_thresholds, dtype=np.float32)
+        rc = nat.lib().artea_gpu_router_set_early_stop(self._h, nat.ptr(thr), thr.size)
+        if rc == nat.EINVAL:
+            msg = nat.lib().artea_gpu_last_error().decode(errors="replace")
+            if "not representable" in msg:
+                raise OverflowError(msg)
+        nat.check(rc)
+
     def set_phase_buffer(self, d_buf) -> None:
         """Record per-query phase cycles into d_buf (device, nq x 8 int64) or stop (None)."""
         nat.check(nat.lib().artea_gpu_router_set_phase_buffer(self._h, nat.ptr(d_buf)))
@@ -240,14 +256,38 @@ class HierarchicalGraphRouter:
         self._cache[key] = (weakref.ref(graph), router)
         return router
 
-    def batch_query(self, query_vecs: np.ndarray, graph: CompactHierarchicalGraph) -> np.ndarray:
-        """knn_results_t: (nq * topk,) uint64 CandidateEntry words."""
-        out = self._router_for(graph).batch_query(query_vecs)
+    def _early_stop(self, router: GpuRouter, graph: CompactHierarchicalGraph, enable_early_stop: bool,
+                    rgraph_config, pruning_config) -> None:
+        """_early_stop_thresholds (hierarchical_graph_router.hpp:388-408): one
+        rgraph_config.early_stop_threshold(h, pruning_config) per upper level,
+        converted and validated by the native router."""
+        if not enable_early_stop:
+            router.set_early_stop(None)
+            return
+        top = graph.top_occupied_level_id()
+        if graph.num_vertices == 0 or top == INVALID_LEVEL or top == 0:
+            router.set_early_stop(None)
+            return
+        if rgraph_config is None or pruning_config is None:
+            raise TypeError("early stopping on a bare graph requires explicit rgraph and pruning configs")
+        thr = [0.0] + [float(rgraph_config.early_stop_threshold(h, pruning_config)) for h in range(1, top + 1)]
+        router.set_early_stop(thr)
+
+    def batch_query(self, query_vecs: np.ndarray, graph: CompactHierarchicalGraph, rgraph_config=None,
+                    pruning_config=None, enable_early_stop: bool = False) -> np.ndarray:
+        """knn_results_t: (nq * topk,) uint64 CandidateEntry words. With
+        enable_early_stop, the config overload (hierarchical_graph_router.hpp:308-319)."""
+        r = self._router_for(graph)
+        self._early_stop(r, graph, enable_early_stop, rgraph_config, pruning_config)
+        out = r.batch_query(query_vecs)
         return out.reshape(-1)
 
-    def query(self, query_vec: np.ndarray, graph: CompactHierarchicalGraph) -> np.ndarray:
+    def query(self, query_vec: np.ndarray, graph: CompactHierarchicalGraph, rgraph_config=None,
+              pruning_config=None, enable_early_stop: bool = False) -> np.ndarray:
         """query(): at most topk entries (the invalid tail is dropped)."""
-        words = self._router_for(graph).batch_query(np.asarray(query_vec, dtype=np.float32).reshape(1, -1))[0]
+        r = self._router_for(graph)
+        self._early_stop(r, graph, enable_early_stop, rgraph_config, pruning_config)
+        words = r.batch_query(np.asarray(query_vec, dtype=np.float32).reshape(1, -1))[0]
         return words[~entry_is_invalid(words)]
 
     def batch_query_l0_only(self, query_vecs: np.ndarray, graph: CompactHierarchicalGraph) -> np.ndarray:

@@ -266,6 +266,170 @@ def run_reference_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def time_steps(router, d_q, nq, k_stride, d_out, d_topk, d_queue, stream, steps, warmup, flush):
+    """CUDA-event time (ms) of each of `steps` launches after `warmup` untimed ones;
+    the L2 flush between steps is outside the events."""
+    import torch
+    for _ in range(warmup):
+        router.batch_query_device(d_q, nq, k_stride, d_out, d_topk=d_topk, d_queue=d_queue, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    ev = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        router.batch_query_device(d_q, nq, k_stride, d_out, d_topk=d_topk, d_queue=d_queue, stream=stream.cuda_stream)
+        e1.record(stream)
+        ev.append((e0, e1))
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def run_uneven(args, w, base, queries, hgra, report, index, device, metric, cache_dir, rank, world):
+    """One launch over queries with uneven per-query topk/queue: the persistent
+    schedule (autotuned, work stealing, CUDA graphs) against the plain
+    one-CTA-per-query schedule; both must return identical words."""
+    import torch
+    from artea_b200.router import GpuRouter
+    nq, dim = queries.shape
+    topk, queue = ds.per_query_params(w, nq)
+    kmax = int(topk.max())
+    gt = ground_truth(base, queries, kmax, w.metric, device, cache_dir)
+    d_q = torch.from_numpy(queries).to(device)
+    d_tk = torch.from_numpy(topk.view(np.int32)).to(device)
+    d_qu = torch.from_numpy(queue.view(np.int32)).to(device)
+    d_out = torch.empty((nq, kmax), dtype=torch.int64, device=device)
+    d_stats = torch.zeros((nq, 8), dtype=torch.int32, device=device)
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    res = {}
+    for sched in ("persistent", "plain"):
+        r = GpuRouter(index, metric, kmax, int(queue.max()), mode=args.mode, schedule=sched, max_batch=nq,
+                      use_graphs=not args.no_graphs)
+        r.batch_query_device(d_q, nq, kmax, d_out, d_topk=d_tk, d_queue=d_qu, d_stats=d_stats,
+                             stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        words = d_out.cpu().numpy().view(np.uint64).copy()
+        stats = d_stats.cpu().numpy().view(np.uint32).copy()
+        l0 = r.launches()
+        with ClockSampler(local_gpu(device)) as clocks:
+            time.sleep(0.3)
+            t0 = time.time()
+            ms = time_steps(r, d_q, nq, kmax, d_out, d_tk, d_qu, stream, args.steps, args.warmup, flush)
+            clocks.mark(t0, time.time())
+            time.sleep(0.2)
+        r.sync()
+        res[sched] = {"ms": statistics.mean(ms), "qps": nq / (statistics.mean(ms) / 1e3),
+                      "recall": recall(words, gt, topk), "tuning": r.tuning(),
+                      "launches": r.launches() - l0 - args.warmup, "stats": stats, "words": words,
+                      "clocks": clocks.summary(), "router": r}
+        log(f"{sched}: {res[sched]['qps']:.0f} q/s, recall {res[sched]['recall']:.5f}, tuning {r.tuning()}")
+    assert np.array_equal(res["persistent"]["words"], res["plain"]["words"]), "schedules disagree"
+    p = res["persistent"]
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        p["router"].batch_query(queries, topk=topk, queue=queue, k_stride=kmax)
+        if i >= args.warmup:
+            e2e.append(time.perf_counter() - t0)
+    alg = float(algorithmic_bytes(p["stats"], dim, topk).sum())
+    peaks = measured_peaks()
+    achieved = alg / (p["ms"] / 1e3) / 1e9
+    baseline = None
+    if not args.no_cpu_baseline:
+        baseline = cpu_baseline_uneven(hgra, base, queries, topk, queue, metric, min(args.cpu_sample, nq))
+    st = p["stats"].astype(np.float64)
+    line = {
+        "metric": METRIC_NAME, "value": p["qps"], "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": p["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w.name, "n_base": w.n_base, "n_query": nq, "dim": dim, "metric": w.metric,
+                   "topk": "per query in {10,100}", "queue": "per query in {64,128,256,512}",
+                   "mode": args.mode, "schedule": "persistent (autotuned, work stealing)",
+                   "cuda_graphs": not args.no_graphs, "recall_at_k": round(p["recall"], 5),
+                   "tuning": p["tuning"], "graph_levels": report.get("vertices_by_highest_level"),
+                   "graph_build_s": report.get("build_s"),
+                   "l2": "256 MiB buffer written between timed steps (excluded from timing)"},
+        "plain_one_cta_per_query": {"qps": res["plain"]["qps"], "ms_per_step": res["plain"]["ms"],
+                                    "recall_at_k": round(res["plain"]["recall"], 5),
+                                    "clocks": res["plain"]["clocks"]},
+        "speedup_vs_plain": p["qps"] / res["plain"]["qps"],
+        "e2e": {"value": nq / statistics.mean(e2e), "unit": "queries/s",
+                "h2d_bytes_per_step": int(queries.nbytes + topk.nbytes + queue.nbytes),
+                "d2h_bytes_per_step": int(nq * kmax * 8)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic(w.name),
+                     "algorithmic_bytes_per_launch": alg, "peak_source": peaks["source"],
+                     "kernel": "search_persistent_kernel"},
+        "cpu_baseline": baseline, "gpu_launches": int(p["launches"]), "clocks": p["clocks"],
+        "per_query": {"dist_evals": float(st[:, 0].mean()), "l0_rows": float(st[:, 3].mean()),
+                      "upper_rows": float(st[:, 1].mean())},
+    }
+    for sched in res:
+        res[sched]["router"].close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_uneven(hgra, base, queries, topk, queue, metric, sample):
+    """The reference router takes one (topk, queue) per instance: the sample is
+    grouped by (topk, queue) and each group runs as one batch_query."""
+    groups = {}
+    for i in range(sample):
+        groups.setdefault((int(topk[i]), int(queue[i])), []).append(i)
+    total, info = 0.0, None
+    for (k, L), idx in sorted(groups.items()):
+        info = cpu_baseline(hgra, base, queries[idx], k, L, metric, len(idx))
+        total += info["seconds_per_run"]
+    return {"value": sample / total, "unit": "queries/s", "cores": info["cores"], "kind": info["kind"],
+            "sample": f"{sample} queries in {len(groups)} (topk, queue) groups, one batch_query per group"}
+
+
+def run_serving(args, w, base, queries, report, index, device, metric, cache_dir):
+    """Serving loop under Poisson arrivals against one batch_query per request."""
+    from artea_b200.router import GpuRouter
+    from artea_b200.serving import Server, make_requests, run_per_batch, run_poisson
+    nq = min(args.serve_queries, queries.shape[0])
+    qs = queries[:nq]
+    gt = ground_truth(base, queries, 100, w.metric, device, cache_dir)[:nq]
+    rates = [float(x) for x in args.serve_rates.split(",") if x]
+    srv = Server(index, metric, max_topk=100, max_queue=400, ring_slots=16384, mode=args.mode)
+    points = []
+    for rate in rates:
+        reqs = make_requests(nq, rate, seed=int(rate))
+        st = run_poisson(srv, qs, reqs, 100)
+        order = sorted(reqs, key=lambda r: r.lo)
+        words = np.vstack([r.result for r in order])
+        ks = np.concatenate([r.topk for r in order])
+        st["recall_at_k"] = round(recall(words, gt, ks), 5)
+        st["offered_qps"] = rate
+        points.append(st)
+        log(f"serving at {rate:.0f} q/s: {st}")
+    sstats = srv.stats()
+    srv.close()
+    router = GpuRouter(index, metric, 100, 400, mode=args.mode, schedule="plain", max_batch=256, max_queue=400)
+    base_pts = []
+    for rate in rates:
+        reqs = make_requests(nq, rate, seed=int(rate))
+        st = run_per_batch(router, qs, reqs, 100)
+        st["offered_qps"] = rate
+        base_pts.append(st)
+        log(f"per-batch launches at {rate:.0f} q/s: {st}")
+    router.close()
+    line = {"metric": "serving p50/p95/p99 latency (ms) and QPS at offered load", "unit": "ms", "n_gpus": 1,
+            "higher_is_better": False, "data": "synthetic", "dtype": "f32",
+            "config": {"workload": w.name, "n_base": w.n_base, "dim": w.dim, "metric": w.metric,
+                       "queries_per_rate": nq, "request_size": "log-uniform [1,256]",
+                       "topk": "{10,100} per request", "queue": "{100,200,400} per request", "mode": args.mode,
+                       "ring_slots": 16384, "arrivals": "Poisson"},
+            "serving": points, "server_stats": sstats, "per_batch_launch": base_pts}
+    print(json.dumps(line), flush=True)
+
+
+def local_gpu(device) -> int:
+    return device.index if getattr(device, "index", None) is not None else 0
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -292,6 +456,14 @@ def main() -> None:
     ap.add_argument("--profile-vh-bits", type=int, default=-1, help="-1: no shared-memory visited hash")
     ap.add_argument("--profile-regs", type=int, default=85)
     ap.add_argument("--phases", action="store_true", help="with --profile: per-phase cycle breakdown")
+    ap.add_argument("--uneven", action="store_true",
+                    help="per-query topk in {10,100} and queue in {64,128,256,512} in one launch (the default for "
+                         "the deep10m workload); compares the persistent and plain schedules")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving loop under Poisson arrivals (request sizes log-uniform in [1,256], topk in "
+                         "{10,100}, queue in {100,200,400}) against one batch_query launch per request")
+    ap.add_argument("--serve-rates", default="1000,10000,50000,100000,200000")
+    ap.add_argument("--serve-queries", type=int, default=20000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -349,6 +521,14 @@ def main() -> None:
                               "phase_share": {n: float(mean[i] / mean[6]) for i, n in enumerate(names[:6])},
                               "tuning": r.tuning()}), flush=True)
         r.close()
+        index.close()
+        return
+    if args.serve:
+        run_serving(args, w, base, queries, report, index, device, metric, cache_dir)
+        index.close()
+        return
+    if args.uneven or w.kind == "deep":
+        run_uneven(args, w, base, queries, hgra, report, index, device, metric, cache_dir, rank, world)
         index.close()
         return
     gt = ground_truth(base, queries, k, w.metric, device, cache_dir) if rank == 0 else None

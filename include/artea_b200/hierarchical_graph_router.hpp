@@ -99,22 +99,70 @@ public:
 
     /** batch_query<RandomSeeding, enable_early_stop>(query_vecs, graph)
      *  (hierarchical_graph_router.hpp:293-349): nq*topk entries, row-major,
-     *  invalid-filled past each query's results. */
+     *  invalid-filled past each query's results. With enable_early_stop the
+     *  graph must carry its configurations, as in the reference (:176-182). */
     template <bool RandomSeeding = false, bool enable_early_stop = false, typename HierarchicalGraphT>
     auto batch_query(const query_vecs_t& query_vecs, const HierarchicalGraphT& hier_graph) const -> knn_results_t {
         static_assert(!RandomSeeding, "the GPU router seeds from the graph's entry point (RandomSeeding=false)");
-        static_assert(!enable_early_stop, "upper-level early stopping is not offered by the GPU router");
         static_assert(HierarchicalGraphT::is_compacted, "the GPU router searches compact graphs");
-        return _run(query_vecs.get_all(), query_vecs.get_num_vecs(), hier_graph, false);
+        if constexpr (enable_early_stop) {
+            static_assert(requires { hier_graph.rgraph_config(); hier_graph.pruning_config(); },
+                          "Early stopping on a bare graph requires explicit rgraph and pruning configs");
+            return batch_query<RandomSeeding, true>(query_vecs, hier_graph, hier_graph.rgraph_config(),
+                                                    hier_graph.pruning_config());
+        } else {
+            return _run(query_vecs.get_all(), query_vecs.get_num_vecs(), hier_graph, false, {});
+        }
+    }
+
+    /** The explicit-config overload (hierarchical_graph_router.hpp:308-319):
+     *  with enable_early_stop, the greedy walk on level h >= 1 stops once its
+     *  cursor is within rgraph_config.early_stop_threshold(h, pruning_config),
+     *  evaluated once per level per call (:388-408; squared for EUCLIDEAN_SQR
+     *  by the library). Throws std::overflow_error when a threshold is not
+     *  representable in query distance units. Without it the configs are not
+     *  read. */
+    template <bool RandomSeeding = false, bool enable_early_stop = false, typename HierarchicalGraphT,
+              typename RGraphConfigT, typename PruningConfigT>
+    auto batch_query(const query_vecs_t& query_vecs, const HierarchicalGraphT& hier_graph,
+                     const RGraphConfigT& rgraph_config, const PruningConfigT& pruning_config) const
+        -> knn_results_t {
+        static_assert(!RandomSeeding, "the GPU router seeds from the graph's entry point (RandomSeeding=false)");
+        static_assert(HierarchicalGraphT::is_compacted, "the GPU router searches compact graphs");
+        if constexpr (enable_early_stop) {
+            return _run(query_vecs.get_all(), query_vecs.get_num_vecs(), hier_graph, false,
+                        _config_thresholds(hier_graph, rgraph_config, pruning_config));
+        } else {
+            return _run(query_vecs.get_all(), query_vecs.get_num_vecs(), hier_graph, false, {});
+        }
     }
 
     /** query(query_vec, graph): at most topk entries (hierarchical_graph_router.hpp:164-174). */
     template <bool RandomSeeding = false, bool enable_early_stop = false, typename HierarchicalGraphT>
     auto query(const vec_ele_t* query_vec, const HierarchicalGraphT& hier_graph) const -> knn_results_t {
-        static_assert(!RandomSeeding && !enable_early_stop, "see batch_query");
-        auto res = _run(query_vec, 1, hier_graph, false);
-        while (!res.empty() && res.back().is_invalid()) res.pop_back();
-        return res;
+        static_assert(!RandomSeeding, "see batch_query");
+        if constexpr (enable_early_stop) {
+            static_assert(requires { hier_graph.rgraph_config(); hier_graph.pruning_config(); },
+                          "Early stopping on a bare graph requires explicit rgraph and pruning configs");
+            return query<RandomSeeding, true>(query_vec, hier_graph, hier_graph.rgraph_config(),
+                                              hier_graph.pruning_config());
+        } else {
+            return _trim(_run(query_vec, 1, hier_graph, false, {}));
+        }
+    }
+
+    /** query with explicit configurations (hierarchical_graph_router.hpp:176-190). */
+    template <bool RandomSeeding = false, bool enable_early_stop = false, typename HierarchicalGraphT,
+              typename RGraphConfigT, typename PruningConfigT>
+    auto query(const vec_ele_t* query_vec, const HierarchicalGraphT& hier_graph, const RGraphConfigT& rgraph_config,
+               const PruningConfigT& pruning_config) const -> knn_results_t {
+        static_assert(!RandomSeeding, "see batch_query");
+        if constexpr (enable_early_stop) {
+            return _trim(_run(query_vec, 1, hier_graph, false,
+                              _config_thresholds(hier_graph, rgraph_config, pruning_config)));
+        } else {
+            return _trim(_run(query_vec, 1, hier_graph, false, {}));
+        }
     }
 
     /** batch_query_l0_only (hierarchical_graph_router.hpp:353-385). */
@@ -123,11 +171,12 @@ public:
         -> knn_results_t {
         static_assert(!RandomSeeding, "see batch_query");
         static_assert(HierarchicalGraphT::is_compacted, "batch_query_l0_only is only defined for compact graphs.");
-        return _run(query_vecs.get_all(), query_vecs.get_num_vecs(), hier_graph, true);
+        return _run(query_vecs.get_all(), query_vecs.get_num_vecs(), hier_graph, true, {});
     }
 
 private:
     struct Device {
+        std::mutex mu;   // early-stop setting + launch of one call
         artea_gpu_index* index = nullptr;
         artea_gpu_router* router = nullptr;
         ~Device() {
@@ -186,10 +235,36 @@ private:
         return ref;
     }
 
+    // Per-level configuration thresholds, index = level, for levels 1..top of
+    // g (empty when g has no level above 0: none is needed, :392-393).
+    template <typename HierarchicalGraphT, typename RGraphConfigT, typename PruningConfigT>
+    static auto _config_thresholds(const HierarchicalGraphT& g, const RGraphConfigT& rgraph_config,
+                                   const PruningConfigT& pruning_config) -> std::vector<float> {
+        const auto top = g.top_occupied_level_id();
+        if (top == HierarchicalGraphT::invalid_level_id || top == 0) return {};
+        std::vector<float> thr(static_cast<std::size_t>(top) + 1, 0.0f);
+        for (uint32_t h = 1; h <= static_cast<uint32_t>(top); ++h)
+            thr[h] = static_cast<float>(rgraph_config.early_stop_threshold(h, pruning_config));
+        return thr;
+    }
+
+    static auto _trim(knn_results_t res) -> knn_results_t {
+        while (!res.empty() && res.back().is_invalid()) res.pop_back();
+        return res;
+    }
+
     template <typename HierarchicalGraphT>
-    auto _run(const vec_ele_t* queries, uint32_t nq, const HierarchicalGraphT& g, bool l0_only) const
-        -> knn_results_t {
+    auto _run(const vec_ele_t* queries, uint32_t nq, const HierarchicalGraphT& g, bool l0_only,
+              const std::vector<float>& early_stop) const -> knn_results_t {
         Device& dev = _device_for(g);
+        std::lock_guard<std::mutex> lk(dev.mu);
+        const int es = early_stop.empty()
+                           ? artea_gpu_router_set_early_stop(dev.router, nullptr, 0)
+                           : artea_gpu_router_set_early_stop(dev.router, early_stop.data(),
+                                                             static_cast<uint32_t>(early_stop.size()));
+        if (es != ARTEA_GPU_OK && std::string(artea_gpu_last_error()).find("not representable") != std::string::npos)
+            throw std::overflow_error(artea_gpu_last_error());
+        detail::check(es, "artea_gpu_router_set_early_stop");
         knn_results_t results(static_cast<std::size_t>(nq) * _topk, candidate_entry_t::make_invalid_entry());
         if (nq == 0 || _topk == 0) return results;
         std::vector<uint64_t> words(static_cast<std::size_t>(nq) * _topk);

@@ -210,6 +210,22 @@ int artea_gpu_router_sync(artea_gpu_router* router);
 /* Number of kernel launches this router has issued (for launch accounting). */
 int artea_gpu_router_launches(const artea_gpu_router* router, uint64_t* launches);
 
+/* Early stop of the upper-level greedy walks: batch_query<RandomSeeding=false,
+ * enable_early_stop=true> (hierarchical_graph_router.hpp:176-190, :308-319;
+ * thresholds :388-408; the stop test detail/beam_loop.hpp:147-150).
+ * level_thresholds[h], h in [1, top], is the graph configuration's
+ * early_stop_threshold(h, pruning_config) in its own distance units (index 0
+ * is not read); for an EUCLIDEAN_SQR router it is squared, as the reference
+ * does. A walk on level h stops once its cursor is at distance <= the
+ * threshold; level 0 never stops early. The setting applies to every later
+ * launch of this router. level_thresholds NULL (or n_levels 0) switches early
+ * stop off. Returns EINVAL when n_levels <= top, or, with the reference's
+ * std::overflow_error text "Early-stop threshold is not representable in query
+ * distance units", when a converted threshold is non-finite, <= 0, above
+ * FLT_MAX or rounds to 0. Graphs that are empty or have no level above 0 need
+ * no thresholds (any array is accepted). */
+int artea_gpu_router_set_early_stop(artea_gpu_router* router, const float* level_thresholds, uint32_t n_levels);
+
 /* Profiling hook: when d_phase_cycles (device memory, nq x 8 uint64) is set,
  * every later launch writes per-query SM clock cycles spent in: greedy upper
  * levels, pop/row lookup, row ids + visited, distances, queue merge, tail,

@@ -15,6 +15,7 @@
 
 #define VID_MASK 0x7FFFFFFFu
 #define INVALID_LEVEL 0xFFFFFFFFu
+#define ORACLE_MAX_LEVELS 64
 
 /* ---------------------------------------------------------------------------
  * Distances: utils/simd_distance.hpp:64-79 (dispatch), 100-115 + 198 (L2^2,
@@ -208,6 +209,7 @@ typedef struct ctx {
     visited vis;
     queue q;
     oracle_stats st;
+    const float* es_thr;   /* per-level early-stop thresholds (query units) or NULL */
 } ctx;
 
 static float dist_of(ctx* c, const float* query, uint32_t vid) {
@@ -222,6 +224,8 @@ static void greedy(ctx* c, const float* query, uint32_t level, uint32_t* cur, fl
     uint32_t best = *cur;
     float best_d = *cur_dist;
     for (;;) {
+        /* enable_early_stop: detail/beam_loop.hpp:147-150 (inclusive). */
+        if (c->es_thr && best_d <= c->es_thr[level]) break;
         uint32_t next = best;
         float next_d = best_d;
         uint32_t len;
@@ -315,6 +319,7 @@ typedef struct job {
     uint64_t* out;
     oracle_stats* stats;
     volatile uint32_t next;
+    const float* es_thr;
 } job;
 
 static uint64_t invalid_word(void) {
@@ -328,7 +333,7 @@ static void* worker(void* arg) {
     job* j = (job*)arg;
     ctx c;
     memset(&c, 0, sizeof(c));
-    c.g = j->g; c.vecs = j->vecs; c.dim = j->dim; c.metric = j->metric;
+    c.g = j->g; c.vecs = j->vecs; c.dim = j->dim; c.metric = j->metric; c.es_thr = j->es_thr;
     c.vis.n = j->g->num_vertices;
     c.vis.tags = (uint16_t*)calloc(c.vis.n ? c.vis.n : 1, sizeof(uint16_t));
     c.vis.version = 1;
@@ -348,14 +353,15 @@ static void* worker(void* arg) {
     return NULL;
 }
 
-int oracle_batch_query(const oracle_graph* g, const float* vecs, uint32_t dim,
-                       const float* queries, uint32_t nq,
-                       const uint32_t* topk, const uint32_t* queue, uint32_t k_stride,
-                       int metric, int l0_only, uint64_t* out, oracle_stats* stats, int threads) {
+static int run_batch(const oracle_graph* g, const float* vecs, uint32_t dim,
+                     const float* queries, uint32_t nq,
+                     const uint32_t* topk, const uint32_t* queue, uint32_t k_stride,
+                     int metric, int l0_only, uint64_t* out, oracle_stats* stats, int threads,
+                     const float* es_thr) {
     if (!g || !out || (nq && (!queries || !topk || !queue)) || dim == 0 || dim % 16) return -1;
     for (uint32_t i = 0; i < nq; ++i)
         if (topk[i] > k_stride || queue[i] < topk[i]) return -1;
-    job j = {g, vecs, dim, queries, nq, topk, queue, k_stride, metric, l0_only, out, stats, 0};
+    job j = {g, vecs, dim, queries, nq, topk, queue, k_stride, metric, l0_only, out, stats, 0, es_thr};
     if (threads < 1) threads = 1;
     if ((uint32_t)threads > nq) threads = nq ? (int)nq : 1;
     pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * threads);
@@ -364,6 +370,41 @@ int oracle_batch_query(const oracle_graph* g, const float* vecs, uint32_t dim,
     for (int t = 1; t < threads; ++t) pthread_join(th[t], NULL);
     free(th);
     return 0;
+}
+
+int oracle_batch_query(const oracle_graph* g, const float* vecs, uint32_t dim,
+                       const float* queries, uint32_t nq,
+                       const uint32_t* topk, const uint32_t* queue, uint32_t k_stride,
+                       int metric, int l0_only, uint64_t* out, oracle_stats* stats, int threads) {
+    return run_batch(g, vecs, dim, queries, nq, topk, queue, k_stride, metric, l0_only, out, stats, threads, NULL);
+}
+
+/* _early_stop_thresholds: hierarchical_graph_router.hpp:388-408. */
+int oracle_early_stop_thresholds(const oracle_graph* g, int metric, const float* cfg, uint32_t n_levels,
+                                 float* out) {
+    const uint32_t top = g->top_level;
+    if (g->num_vertices == 0 || top == INVALID_LEVEL || top == 0) return 0;
+    if (!cfg || n_levels <= top) return -1;
+    out[0] = 0.0f;
+    for (uint32_t h = 1; h <= top; ++h) {
+        double t = (double)cfg[h];
+        if (metric == ORACLE_EUCLIDEAN_SQR) t *= t;
+        if (!isfinite(t) || t <= 0.0 || t > (double)FLT_MAX || (float)t == 0.0f) return -2;
+        out[h] = (float)t;
+    }
+    return 0;
+}
+
+int oracle_batch_query_early_stop(const oracle_graph* g, const float* vecs, uint32_t dim,
+                                  const float* queries, uint32_t nq,
+                                  const uint32_t* topk, const uint32_t* queue, uint32_t k_stride,
+                                  int metric, const float* cfg_thresholds, uint32_t n_levels,
+                                  uint64_t* out, oracle_stats* stats, int threads) {
+    float thr[ORACLE_MAX_LEVELS] = {0};
+    if (!g || (g->top_level >= ORACLE_MAX_LEVELS && g->top_level != INVALID_LEVEL)) return -1;
+    const int rc = oracle_early_stop_thresholds(g, metric, cfg_thresholds, n_levels, thr);
+    if (rc != 0) return rc;
+    return run_batch(g, vecs, dim, queries, nq, topk, queue, k_stride, metric, 0, out, stats, threads, thr);
 }
 
 /* ---------------------------------------------------------------------------

@@ -60,6 +60,25 @@ int oracle_batch_query(const oracle_graph* g, const float* vecs, uint32_t dim,
                        const uint32_t* topk, const uint32_t* queue, uint32_t k_stride,
                        int metric, int l0_only, uint64_t* out, oracle_stats* stats, int threads);
 
+/* _early_stop_thresholds (hierarchical_graph_router.hpp:388-408): out[h] for
+ * h in [1, top] from the configuration's per-level thresholds cfg[h] (squared
+ * for EUCLIDEAN_SQR). Returns 0, -1 when cfg covers no more than levels
+ * [0, top], -2 when a threshold is not representable in query units (the
+ * reference's std::overflow_error). Empty or level-0-only graphs need none. */
+int oracle_early_stop_thresholds(const oracle_graph* g, int metric, const float* cfg, uint32_t n_levels,
+                                 float* out);
+
+/* batch_query<RandomSeeding=false, enable_early_stop=true>
+ * (hierarchical_graph_router.hpp:308-319): as oracle_batch_query, with the
+ * greedy walk on level h stopping once its cursor distance is <= the level's
+ * threshold (detail/beam_loop.hpp:147-150). Returns the codes of
+ * oracle_early_stop_thresholds, or -1 on a bad argument. */
+int oracle_batch_query_early_stop(const oracle_graph* g, const float* vecs, uint32_t dim,
+                                  const float* queries, uint32_t nq,
+                                  const uint32_t* topk, const uint32_t* queue, uint32_t k_stride,
+                                  int metric, const float* cfg_thresholds, uint32_t n_levels,
+                                  uint64_t* out, oracle_stats* stats, int threads);
+
 /* Exact top-k by (distance, vid) over all vectors: ground truth. */
 int oracle_bruteforce(const float* vecs, uint32_t n, uint32_t dim, const float* queries, uint32_t nq,
                       uint32_t k, int metric, uint32_t* out_ids, float* out_dists, int threads);

@@ -53,6 +53,10 @@ def oracle_lib():
         L.oracle_batch_query.restype = c_int
         L.oracle_batch_query.argtypes = [POINTER(_Graph), c_void_p, c_uint32, c_void_p, c_uint32, c_void_p, c_void_p,
                                          c_uint32, c_int, c_int, c_void_p, c_void_p, c_int]
+        L.oracle_batch_query_early_stop.restype = c_int
+        L.oracle_batch_query_early_stop.argtypes = [POINTER(_Graph), c_void_p, c_uint32, c_void_p, c_uint32, c_void_p,
+                                                    c_void_p, c_uint32, c_int, c_void_p, c_uint32, c_void_p, c_void_p,
+                                                    c_int]
         L.oracle_bruteforce.restype = c_int
         L.oracle_bruteforce.argtypes = [c_void_p, c_uint32, c_uint32, c_void_p, c_uint32, c_uint32, c_int, c_void_p,
                                         c_void_p, c_int]
@@ -77,6 +81,9 @@ def ref_lib():
         L.artea_ref_batch_query.restype = c_int
         L.artea_ref_batch_query.argtypes = [c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_int, c_int, c_int,
                                             c_void_p, POINTER(c_double), c_void_p]
+        L.artea_ref_batch_query_early_stop.restype = c_int
+        L.artea_ref_batch_query_early_stop.argtypes = [c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_int,
+                                                       c_void_p, c_uint32, c_void_p, c_void_p]
         L.artea_ref_distance.restype = c_float
         L.artea_ref_distance.argtypes = [c_int, c_void_p, c_void_p, c_uint32]
         L.artea_ref_max_threads.restype = c_int
@@ -100,12 +107,17 @@ def ref_distance(metric: int, a: np.ndarray, b: np.ndarray) -> float:
     return float(ref_lib().artea_ref_distance(metric, _p(a), _p(b), a.size))
 
 
+class EarlyStopNotRepresentable(OverflowError):
+    """The reference's std::overflow_error from _early_stop_thresholds."""
+
+
 def batch_query(graph, base: np.ndarray, queries: np.ndarray, topk, queue, metric: int = 0, l0_only: bool = False,
-                k_stride: int = None, threads: int = None, stats: bool = False):
+                k_stride: int = None, threads: int = None, stats: bool = False, early_stop=None):
     """C restatement of batch_query; graph is an artea_b200.graph.CompactHierarchicalGraph.
 
-    topk/queue: ints or per-query arrays. Returns (nq, k_stride) uint64 words
-    and, if stats, an (nq, 8) uint32 counter array."""
+    topk/queue: ints or per-query arrays. early_stop: per-level configuration
+    thresholds (index = level) for enable_early_stop=true, or None. Returns
+    (nq, k_stride) uint64 words and, if stats, an (nq, 8) uint32 counter array."""
     base = np.ascontiguousarray(base, dtype=np.float32)
     q = np.ascontiguousarray(queries, dtype=np.float32)
     nq = q.shape[0]
@@ -123,8 +135,18 @@ def batch_query(graph, base: np.ndarray, queries: np.ndarray, topk, queue, metri
                ctypes.cast(offs, POINTER(POINTER(c_uint64))),
                graph.neighbor_ids.ctypes.data_as(POINTER(c_uint32)))
     threads = threads or os.cpu_count() or 1
-    rc = oracle_lib().oracle_batch_query(ctypes.byref(g), _p(base), base.shape[1], _p(q), nq, _p(tk), _p(qu),
-                                         k_stride, metric, 1 if l0_only else 0, _p(out), _p(st), threads)
+    if early_stop is not None:
+        if l0_only:
+            raise ValueError("early stop applies to the hierarchical query only")
+        thr = np.ascontiguousarray(early_stop, dtype=np.float32)
+        rc = oracle_lib().oracle_batch_query_early_stop(ctypes.byref(g), _p(base), base.shape[1], _p(q), nq, _p(tk),
+                                                        _p(qu), k_stride, metric, _p(thr), thr.size, _p(out), _p(st),
+                                                        threads)
+        if rc == -2:
+            raise EarlyStopNotRepresentable("Early-stop threshold is not representable in query distance units")
+    else:
+        rc = oracle_lib().oracle_batch_query(ctypes.byref(g), _p(base), base.shape[1], _p(q), nq, _p(tk), _p(qu),
+                                             k_stride, metric, 1 if l0_only else 0, _p(out), _p(st), threads)
     if rc != 0:
         raise ValueError("oracle_batch_query rejected its arguments")
     return (out, st) if stats else out
@@ -165,6 +187,22 @@ class RefRouter:
         if rc != 0:
             raise RuntimeError(ref_lib().artea_ref_last_error().decode())
         return (out, secs.value, calls) if count_distances else (out, secs.value)
+
+    def batch_query_early_stop(self, queries: np.ndarray, topk: int, queue: int, thresholds, metric: int = 0,
+                               count_distances: bool = False):
+        """batch_query<false, true> with per-level configuration thresholds.
+        Returns words (nq, topk) [, dist_calls (nq,)]."""
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        thr = np.ascontiguousarray(thresholds, dtype=np.float32)
+        out = np.empty((q.shape[0], topk), dtype=np.uint64)
+        calls = np.zeros(q.shape[0], dtype=np.uint64) if count_distances else None
+        rc = ref_lib().artea_ref_batch_query_early_stop(self._h, _p(q), q.shape[0], topk, queue, metric, _p(thr),
+                                                        thr.size, _p(out), _p(calls))
+        if rc == -2:
+            raise EarlyStopNotRepresentable(ref_lib().artea_ref_last_error().decode())
+        if rc != 0:
+            raise RuntimeError(ref_lib().artea_ref_last_error().decode())
+        return (out, calls) if count_distances else out
 
     def close(self):
         if self._h:

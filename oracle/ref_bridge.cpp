@@ -15,6 +15,7 @@
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <limits>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -91,6 +92,57 @@ int run(RefIndex& idx, const float* queries, uint32_t nq, uint32_t topk, uint32_
     return 0;
 }
 
+// Per-level thresholds handed to the reference's enable_early_stop overloads
+// (hierarchical_graph_router.hpp:176-190, :308-319) in the shape of the
+// configuration they read (RGraphConfig::early_stop_threshold(h, pruning)).
+struct TableConfig {
+    const float* thr;
+    uint32_t n;
+    auto early_stop_threshold(uint32_t h, const TableConfig&) const -> float {
+        return h < n ? thr[h] : std::numeric_limits<float>::quiet_NaN();
+    }
+};
+
+template <DistanceMetricsT Metric, vec_dim_t Dim>
+int run_early_stop(RefIndex& idx, const float* queries, uint32_t nq, uint32_t topk, uint32_t queue,
+                   const TableConfig& cfg, uint64_t* out, uint64_t* dist_calls) {
+    vector_array_t qv = copy_rows(queries, nq, Dim);
+    using RT = RouterTraits<CountingComputer<Metric, Dim>, index_traits_t, false>;
+    typename RT::dist_func_t dist;
+    typename RT::hierarchical_graph_router_t router(idx.vecs, dist, topk, queue);
+    router.initialize();
+    const auto batch = router.template batch_query<false, true>(qv, idx.graph, cfg, cfg);
+    std::memcpy(out, batch.data(), sizeof(uint64_t) * batch.size());
+    if (dist_calls) {
+        for (uint32_t i = 0; i < nq; ++i) {
+            t_dist_calls = 0;
+            auto r = router.template query<false, true>(qv.get(i), idx.graph, cfg, cfg);
+            dist_calls[i] = t_dist_calls;
+            for (uint32_t j = 0; j < topk; ++j) {
+                const auto e = j < r.size() ? r[j] : RT::candidate_entry_t::make_invalid_entry();
+                uint64_t w;
+                std::memcpy(&w, &e, sizeof(w));
+                if (w != out[std::size_t(i) * topk + j])
+                    throw std::logic_error("reference query and batch_query disagree under early stop");
+            }
+        }
+    }
+    return 0;
+}
+
+template <DistanceMetricsT Metric>
+int by_dim_es(RefIndex& idx, const float* q, uint32_t nq, uint32_t k, uint32_t L, const TableConfig& cfg,
+              uint64_t* out, uint64_t* calls) {
+    switch (idx.vecs.get_vec_dim()) {
+        case 16: return run_early_stop<Metric, 16>(idx, q, nq, k, L, cfg, out, calls);
+        case 96: return run_early_stop<Metric, 96>(idx, q, nq, k, L, cfg, out, calls);
+        case 128: return run_early_stop<Metric, 128>(idx, q, nq, k, L, cfg, out, calls);
+        case 960: return run_early_stop<Metric, 960>(idx, q, nq, k, L, cfg, out, calls);
+        default: break;
+    }
+    throw std::invalid_argument("unsupported padded dim " + std::to_string(idx.vecs.get_vec_dim()));
+}
+
 template <DistanceMetricsT Metric>
 int by_dim(RefIndex& idx, const float* q, uint32_t nq, uint32_t k, uint32_t L, int l0_only, uint64_t* out,
            double* s, uint64_t* calls) {
@@ -140,6 +192,31 @@ int artea_ref_batch_query(void* h, const float* queries, uint32_t nq, uint32_t t
             case 3: return by_dim<DistanceMetricsT::DOT>(idx, queries, nq, topk, queue, l0_only, out, seconds, dist_calls);
             default: throw std::invalid_argument("unknown metric");
         }
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// batch_query<RandomSeeding=false, enable_early_stop=true> with per-level
+// configuration thresholds cfg[0, n_levels). Returns 0, -1 on an error, -2
+// when the reference throws std::overflow_error (threshold not representable).
+int artea_ref_batch_query_early_stop(void* h, const float* queries, uint32_t nq, uint32_t topk, uint32_t queue,
+                                     int metric, const float* cfg, uint32_t n_levels, uint64_t* out,
+                                     uint64_t* dist_calls) {
+    try {
+        auto& idx = *static_cast<RefIndex*>(h);
+        const TableConfig c{cfg, n_levels};
+        switch (metric) {
+            case 0: return by_dim_es<DistanceMetricsT::EUCLIDEAN_SQR>(idx, queries, nq, topk, queue, c, out, dist_calls);
+            case 1: return by_dim_es<DistanceMetricsT::EUCLIDEAN>(idx, queries, nq, topk, queue, c, out, dist_calls);
+            case 2: return by_dim_es<DistanceMetricsT::COSINE>(idx, queries, nq, topk, queue, c, out, dist_calls);
+            case 3: return by_dim_es<DistanceMetricsT::DOT>(idx, queries, nq, topk, queue, c, out, dist_calls);
+            default: throw std::invalid_argument("unknown metric");
+        }
+    } catch (const std::overflow_error& e) {
+        g_last_error = e.what();
+        return -2;
     } catch (const std::exception& e) {
         g_last_error = e.what();
         return -1;

@@ -12,6 +12,7 @@ if ROOT not in sys.path:
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 GOLDEN_CASES = ["early_stop_top0", "early_stop_top2", "early_stop_sqr", "axis80", "sift2k", "deep1k_cos", "gist400"]
+EARLY_STOP_CASES = ["early_stop_top2", "early_stop_sqr", "sift2k", "gist400"]
 BUILDER = os.path.join(ROOT, "index_build", "_ref", "artea_build_index")
 
 
@@ -36,6 +37,14 @@ class Case:
         self.calls = {L: z[f"calls_L{L}"] for L in self.queues}
         self.l0_words = {L: z[f"l0_words_L{L}"] for L in self.queues if f"l0_words_L{L}" in z}
         self.l0_calls = {L: z[f"l0_calls_L{L}"] for L in self.queues if f"l0_calls_L{L}" in z}
+        # enable_early_stop=true outputs: per threshold set i, the configuration
+        # thresholds and the reference's words / distance calls per queue size.
+        self.es = []
+        i = 0
+        while f"es_cfg{i}" in z:
+            self.es.append((z[f"es_cfg{i}"], {L: z[f"es_words{i}_L{L}"] for L in self.queues},
+                            {L: z[f"es_calls{i}_L{L}"] for L in self.queues}))
+            i += 1
         fd, path = tempfile.mkstemp(suffix=".hgra")
         with os.fdopen(fd, "wb") as f:
             f.write(z["hgra"].tobytes())

@@ -6,12 +6,16 @@
 //
 // usage: test_dropin GRAPH.hgra BASE.fbin QUERIES.fbin METRIC TOPK QUEUE
 //        test_dropin --cpu-only     (constructor contract only; no GPU)
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 #include <stdexcept>
 #include <string>
 
 #include <artea/cpu/framework/type_context/default_context.hpp>
+#include <artea/cpu/index/exact_artea/configs.hpp>
 #include <artea_b200/hierarchical_graph_router.hpp>
 
 using namespace artea::cpu;
@@ -39,6 +43,61 @@ bool same(const R& a, const R& b, const char* what) {
     return true;
 }
 
+using rgraph_config_t = index_traits_t::exact_artea::rgraph_config_t;
+using pruning_config_t = index_traits_t::exact_artea::pruning_config_t;
+
+// Per-level thresholds in the shape of an RGraphConfig (early_stop_threshold(h, pruning)).
+struct TableConfig {
+    std::vector<float> t;
+    auto early_stop_threshold(uint32_t h, const pruning_config_t&) const -> float { return t.at(h); }
+};
+
+// enable_early_stop=true through the explicit-config overloads
+// (hierarchical_graph_router.hpp:176-190, :308-319): identical results, and
+// the same std::overflow_error for a threshold that squares past FLT_MAX.
+template <DistanceMetricsT M, typename Cpu, typename Gpu>
+bool early_stop_checks(const Cpu& cpu, const Gpu& gpu, const compact::hierarchical_graph_t& g,
+                       const vector_array_t& base, const vector_array_t& queries) {
+    bool ok = true;
+    const pruning_config_t pruning(2, 0);
+    const rgraph_config_t cfg(2, 0, 0, 1, 4, 4, 4, 4, 4);   // test_router_early_stop.cpp:52-53
+    ok &= same(cpu.template batch_query<false, true>(queries, g, cfg, pruning),
+               gpu.template batch_query<false, true>(queries, g, cfg, pruning), "batch_query early stop (config)");
+    const auto top = g.top_occupied_level_id();
+    if (top == compact::hierarchical_graph_t::invalid_level_id || top == 0) return ok;
+    // Thresholds that stop about half the walks: the median query-to-entry
+    // distance in configuration (L2) units.
+    std::vector<float> d;
+    for (uint32_t i = 0; i < queries.get_num_vecs(); ++i) {
+        double s = 0;
+        for (uint32_t j = 0; j < base.get_vec_dim(); ++j) {
+            const double x = double(queries.get(i)[j]) - double(base.get(g.entry_point_vid())[j]);
+            s += x * x;
+        }
+        d.push_back(static_cast<float>(std::sqrt(s)));
+    }
+    std::sort(d.begin(), d.end());
+    const TableConfig table{std::vector<float>(top + 1, d[d.size() / 2])};
+    ok &= same(cpu.template batch_query<false, true>(queries, g, table, pruning),
+               gpu.template batch_query<false, true>(queries, g, table, pruning), "batch_query early stop (table)");
+    for (uint32_t i = 0; i < queries.get_num_vecs() && i < 8; ++i)
+        ok &= same(cpu.template query<false, true>(queries.get(i), g, table, pruning),
+                   gpu.template query<false, true>(queries.get(i), g, table, pruning), "query early stop");
+    if constexpr (M == DistanceMetricsT::EUCLIDEAN_SQR) {
+        const TableConfig huge{std::vector<float>(top + 1, 1e20f)};
+        int thrown = 0;
+        try { (void)cpu.template batch_query<false, true>(queries, g, huge, pruning); }
+        catch (const std::overflow_error&) { ++thrown; }
+        try { (void)gpu.template batch_query<false, true>(queries, g, huge, pruning); }
+        catch (const std::overflow_error&) { ++thrown; }
+        if (thrown != 2) {
+            std::printf("MISMATCH overflow_error (%d of 2 threw)\n", thrown);
+            ok = false;
+        }
+    }
+    return ok;
+}
+
 template <DistanceMetricsT M, vec_dim_t D>
 int run(const compact::hierarchical_graph_t& g, const vector_array_t& base, const vector_array_t& queries,
         uint32_t topk, uint32_t queue) {
@@ -58,6 +117,10 @@ int run(const compact::hierarchical_graph_t& g, const vector_array_t& base, cons
         ok &= same(cpu.template query<false>(queries.get(i), g), gpu.template query<false>(queries.get(i), g),
                    "query");
     }
+    ok &= early_stop_checks<M>(cpu, gpu, g, base, queries);
+    // back to enable_early_stop=false on the same routers
+    ok &= same(cpu.template batch_query<false>(queries, g), gpu.template batch_query<false>(queries, g),
+               "batch_query after early stop");
     std::printf("%s %zu batch entries compared\n", ok ? "OK" : "FAIL", a.size());
     return ok ? 0 : 1;
 }

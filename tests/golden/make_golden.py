@@ -138,7 +138,68 @@ def built_case(name: str, workload: str, n_base: int, n_query: int, metric_build
               base_dtype=np.uint8 if quantize_u8 else np.float32, l0_only=True)
 
 
+def graph_of(path: str) -> CompactHierarchicalGraph:
+    with tempfile.TemporaryDirectory() as tmp:
+        hgra = os.path.join(tmp, "g.hgra")
+        with open(hgra, "wb") as f:
+            f.write(np.load(path)["hgra"].tobytes())
+        return CompactHierarchicalGraph.from_hgra(hgra)
+
+
+def entry_threshold(path: str, quantile: float) -> float:
+    """A configuration-unit threshold that stops some walks early: the given
+    quantile of the query-to-entry-point distances (square-rooted for L2^2)."""
+    d = np.load(path)
+    g = graph_of(path)
+    base = d["base"].astype(np.float32)
+    metric = int(d["metric"])
+    ent = np.array([orc.ref_distance(metric, q, base[g.entry_point_vid]) for q in d["queries"]], dtype=np.float64)
+    if metric == 0:
+        ent = np.sqrt(ent)
+    return float(np.quantile(ent, quantile))
+
+
+def add_early_stop(name: str, configs) -> None:
+    """Adds, for each per-level configuration threshold array, the reference's
+    batch_query<false, true> words and per-query distance calls at every queue
+    size of the case: keys es_cfg{i}, es_words{i}_L{L}, es_calls{i}_L{L}."""
+    path = os.path.join(HERE, f"{name}.npz")
+    d = dict(np.load(path))
+    for key in [k for k in d if k.startswith("es_")]:
+        del d[key]
+    with tempfile.TemporaryDirectory() as tmp:
+        hgra = os.path.join(tmp, "g.hgra")
+        with open(hgra, "wb") as f:
+            f.write(d["hgra"].tobytes())
+        base = d["base"].astype(np.float32)
+        r = orc.RefRouter(hgra, base)
+        for i, cfg in enumerate(configs):
+            cfg = np.asarray(cfg, dtype=np.float32)
+            d[f"es_cfg{i}"] = cfg
+            for L in d["queues"]:
+                words, calls = r.batch_query_early_stop(d["queries"], int(d["topk"]), int(L), cfg,
+                                                        metric=int(d["metric"]), count_distances=True)
+                d[f"es_words{i}_L{L}"] = words
+                d[f"es_calls{i}_L{L}"] = calls
+        r.close()
+    np.savez_compressed(path, **d)
+    print(name, "early stop:", len(configs), "threshold sets")
+
+
+def early_stop_fixtures() -> None:
+    # test_router_early_stop.cpp:52-53: theta=1 gives gamma=4, T_1=8, T_2=16.
+    add_early_stop("early_stop_top2", [[0, 8, 16], [0, 100, 100], [0, 4, 4]])
+    add_early_stop("early_stop_sqr", [[0, 8, 16], [0, 100, 100], [0, 4, 4]])
+    for name in ("sift2k", "gist400"):
+        path = os.path.join(HERE, f"{name}.npz")
+        top = graph_of(path).top_occupied_level_id()
+        add_early_stop(name, [[0.0] + [entry_threshold(path, q)] * top for q in (0.2, 0.5)])
+
+
 def main() -> None:
+    if "--early-stop-only" in sys.argv:
+        early_stop_fixtures()
+        return
     # Hand-made graphs from the reference unit tests.
     for top in (0, 2):
         save_case(f"early_stop_top{top}", early_stop_graph(top), early_stop_vectors(), early_stop_vectors(),
@@ -150,6 +211,7 @@ def main() -> None:
     built_case("sift2k", "sift100k", 2000, 64, "euclidean", 0, 10, [10, 32, 100], quantize_u8=True)
     built_case("deep1k_cos", "deep10m", 1000, 48, "cosine", 2, 10, [16, 64])
     built_case("gist400", "gist1m", 400, 24, "euclidean", 0, 10, [20, 50], l0=0.05)
+    early_stop_fixtures()
 
 
 if __name__ == "__main__":

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, golden_case
+from conftest import EARLY_STOP_CASES, GOLDEN_CASES, golden_case
 from oracle import oracle as orc
 
 
@@ -116,3 +116,78 @@ def test_recall_estimator_semantics():
     words = np.array([[1, 1, 2], [5, 6, 7]], dtype=np.uint64)
     gt = np.array([[1, 2, 3], [7, 8, 9]], dtype=np.uint32)
     assert orc.recall_at_k(words, gt, 3) == pytest.approx(3 / 6)
+
+
+@pytest.mark.parametrize("name", EARLY_STOP_CASES)
+def test_oracle_early_stop_matches_reference(name):
+    # batch_query<false, true> with per-level configuration thresholds.
+    c = golden_case(name)
+    assert c.es
+    for cfg, words, calls in c.es:
+        for L in c.queues:
+            out, st = orc.batch_query(c.graph, c.base, c.queries, c.topk, L, metric=c.metric, stats=True,
+                                      threads=4, early_stop=cfg)
+            np.testing.assert_array_equal(out, words[L], err_msg=f"{name} cfg={cfg} L={L}")
+            np.testing.assert_array_equal(st[:, 0].astype(np.uint64), calls[L], err_msg=f"{name} L={L} calls")
+
+
+def test_early_stop_known_answer_five_calls():
+    # test_router_early_stop.cpp:121-135: T_1 = 8, T_2 = 16 -> vid 3, distance
+    # 0, 5 distance calls (7 without early stop); L2 and squared L2 alike.
+    for name, metric in (("early_stop_top2", 1), ("early_stop_sqr", 0)):
+        c = golden_case(name)
+        out, st = orc.batch_query(c.graph, c.base, c.queries[3:4], 1, 4, metric=metric, stats=True,
+                                  early_stop=[0, 8, 16])
+        assert (int(out[0, 0]) & 0x7FFFFFFF) == 3
+        assert (int(out[0, 0]) >> 32) == 0
+        assert st[0, 0] == 5
+
+
+def test_early_stop_batch_rows_match_single_queries():
+    # test_router_early_stop.cpp:160-180: batch row i returns vid i.
+    c = golden_case("early_stop_top2")
+    out = orc.batch_query(c.graph, c.base, c.queries, 1, 4, metric=1, early_stop=[0, 8, 16])
+    assert [int(w) & 0x7FFFFFFF for w in out[:, 0]] == [0, 1, 2, 3]
+
+
+def test_early_stop_bottom_only_graph_needs_no_thresholds():
+    # test_router_early_stop.cpp:183-197.
+    c = golden_case("early_stop_top0")
+    out = orc.batch_query(c.graph, c.base, c.queries[3:4], 1, 4, metric=1, early_stop=[])
+    assert (int(out[0, 0]) & 0x7FFFFFFF) == 3
+
+
+@pytest.mark.parametrize("metric,cfg,raises", [
+    (0, [0, 1e20, 1e20], True),      # overflows FLT_MAX once squared
+    (0, [0, 1e-30, 1e-30], True),    # rounds to 0 once squared
+    (0, [0, np.inf, 8], True),
+    (0, [0, 8, -1], False),          # squared first: 1 is representable
+    (1, [0, 8, -1], True),           # L2 keeps the sign: <= 0
+    (1, [0, 0, 8], True),
+    (1, [0, 1e-30, 8], False),       # L2 is not squared
+])
+def test_early_stop_unrepresentable_thresholds(metric, cfg, raises):
+    # test_router_early_stop.cpp:200-210 and hierarchical_graph_router.hpp:398-404:
+    # thresholds that are not positive finite floats in query units (after
+    # squaring for L2^2) raise std::overflow_error; the oracle agrees with the
+    # reference on which ones.
+    c = golden_case("early_stop_sqr" if metric == 0 else "early_stop_top2")
+
+    def outcome(fn):
+        try:
+            fn()
+            return False
+        except orc.EarlyStopNotRepresentable:
+            return True
+
+    assert outcome(lambda: orc.batch_query(c.graph, c.base, c.queries, 1, 4, metric=metric, early_stop=cfg)) == raises
+    if orc.have_ref():
+        r = orc.RefRouter(c.hgra_path, c.base)
+        assert outcome(lambda: r.batch_query_early_stop(c.queries, 1, 4, cfg, metric=metric)) == raises
+        r.close()
+
+
+def test_early_stop_thresholds_shorter_than_the_hierarchy_are_rejected():
+    c = golden_case("early_stop_top2")
+    with pytest.raises(ValueError):
+        orc.batch_query(c.graph, c.base, c.queries, 1, 4, metric=1, early_stop=[0, 8])
