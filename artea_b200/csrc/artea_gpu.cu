@@ -96,6 +96,38 @@ struct artea_gpu_router {
     float es_thr[artea_gpu::kMaxGroups] = {};
 };
 
+namespace artea_gpu {
+
+// Sets *repeat when some level-0 row of at most 64 ids names an id twice; one
+// warp per vertex. Rows without repeats let the search take a whole row in one
+// pass (collect_row64_unique).
+__global__ void l0_rows_repeat_kernel(const unsigned long long* __restrict__ l0row,
+                                      const uint32_t* __restrict__ nbrs, uint32_t n, int* repeat) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+        const unsigned long long d = l0row[v];
+        const uint32_t len = static_cast<uint32_t>(d >> kRowLenShift);
+        if (len > 64u) continue;   // warp-uniform
+        const uint32_t* row = nbrs + (d & kRowStartMask);
+        const bool in0 = lane < len, in1 = lane + 32u < len;
+        const uint32_t x0 = in0 ? row[lane] : 0xffffffffu;
+        const uint32_t x1 = in1 ? row[lane + 32u] : 0xfffffffeu;
+        // Every lane takes part in both matches (a short-circuit here would
+        // leave lanes out of a full-mask warp intrinsic).
+        const uint32_t m0 = __match_any_sync(kFull, x0);
+        const uint32_t m1 = __match_any_sync(kFull, x1);
+        bool dup = (in0 && __popc(m0) > 1) || (in1 && __popc(m1) > 1);
+        for (uint32_t k = 0; k < 32u; ++k) {
+            const uint32_t y = __shfl_sync(kFull, x0, static_cast<int>(k));
+            if (in1 && k < len && y == x1) dup = true;
+        }
+        if (__any_sync(kFull, dup) && lane == 0) atomicOr(repeat, 1);
+    }
+}
+
+}  // namespace artea_gpu
+
 namespace {
 
 using namespace artea_gpu;
@@ -214,6 +246,7 @@ int fill_args(artea_gpu_router* r, SearchArgs* a, const float* d_q, uint32_t nq,
     a->g.dim = ix->dim;
     a->g.top = ix->top;
     a->g.entry = ix->entry;
+    a->g.l0_unique = ix->l0_unique;
     for (int h = 0; h < kMaxGroups; ++h) a->g.offsets[h] = ix->group_ptr[h];
     a->queries = d_q;
     a->nq = nq;
@@ -535,6 +568,17 @@ int artea_gpu_index_create(const artea_gpu_graph_desc* g, const float* vectors, 
             return cleanup(fail(ARTEA_GPU_ECUDA, "row descriptor upload failed"));
         ix->bytes += sizeof(uint2) * ix->n + sizeof(uint32_t) * nn + sizeof(uint64_t) * total +
                      sizeof(unsigned long long) * ix->n;
+        int* d_repeat = nullptr;
+        if (int rc = dev_alloc(&d_repeat, 1)) return cleanup(rc);
+        int repeat = 1;
+        cudaMemset(d_repeat, 0, sizeof(int));
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        artea_gpu::l0_rows_repeat_kernel<<<std::max(sms, 1) * 8, 256>>>(ix->d_l0row, ix->d_nbrs, ix->n, d_repeat);
+        const cudaError_t e = cudaMemcpy(&repeat, d_repeat, sizeof(int), cudaMemcpyDeviceToHost);
+        dev_free(d_repeat);
+        if (e != cudaSuccess) return cleanup(fail(ARTEA_GPU_ECUDA, "row check failed"));
+        ix->l0_unique = repeat ? 0u : 1u;
     }
     *out = ix;
     return ARTEA_GPU_OK;
@@ -911,6 +955,7 @@ extern "C" int artea_gpu_batch_query_noalloc(const artea_gpu_index* ix, int metr
     a.g.dim = ix->dim;
     a.g.top = ix->top;
     a.g.entry = ix->entry;
+    a.g.l0_unique = ix->l0_unique;
     for (int h = 0; h < kMaxGroups; ++h) a.g.offsets[h] = ix->group_ptr[h];
     a.queries = d_queries;
     a.nq = nq;

@@ -55,6 +55,7 @@ struct DeviceGraph {
     uint32_t dim;
     uint32_t top;      // kInvalidLevel when empty
     uint32_t entry;
+    uint32_t l0_unique;   // every level-0 row of <= 64 ids holds distinct ids
     const uint64_t* offsets[kMaxGroups];
 };
 
@@ -208,14 +209,6 @@ __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ 
     const int gi = lane & 3;
     const uint32_t dim = g.dim;
     const uint32_t nchunks = dim >> 4;
-    if (cnt > 8) {
-        // Rows of later passes: one bulk L2 prefetch per row, so those passes
-        // hit L2 instead of paying a full HBM round trip each.
-        for (uint32_t i = 8 + lane; i < cnt; i += 32) {
-            const float* rowp = g.vecs + static_cast<size_t>(cvid[i]) * dim;
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rowp), "r"(dim * 4u) : "memory");
-        }
-    }
     for (uint32_t p = 0; p < cnt; p += 8) {
         const uint32_t idx = p + r;
         const bool valid = idx < cnt;
@@ -355,6 +348,103 @@ __device__ __forceinline__ void visited_set(Visited& vs, uint32_t vid) {
     visited_test_and_set(vs, vid, lane_id() == 0);
 }
 
+// table_test_insert for two distinct ids per lane, the two dependency chains
+// interleaved. r0/r1 as table_test_insert's return values (-1: inactive).
+__device__ __forceinline__ void table_test_insert2(const Visited& vs, uint32_t v0, bool a0, uint32_t v1, bool a1,
+                                                   int* r0, int* r1) {
+    const uint32_t qbits = vs.kbits - vs.tbits;
+    const uint32_t qmask = (1u << qbits) - 1u;
+    const uint32_t p0 = (v0 * kVisitedMul) & vs.kmask, p1 = (v1 * kVisitedMul) & vs.kmask;
+    const uint32_t bk0 = p0 >> qbits, bk1 = p1 >> qbits;
+    const uint32_t q0 = p0 & qmask, q1 = p1 & qmask;
+    const uint32_t pair0 = q0 | (q0 << 16), pair1 = q1 | (q1 << 16);
+    bool pend0 = a0, pend1 = a1;
+    *r0 = a0 ? 2 : -1;
+    *r1 = a1 ? 2 : -1;
+    for (int attempt = 0; attempt < 16 && (pend0 || pend1); ++attempt) {
+        const uint4 b0 = vs.tab[pend0 ? bk0 : 0];
+        const uint4 b1 = vs.tab[pend1 ? bk1 : 0];
+        int wi0 = -1, wi1 = -1;
+        uint32_t old0 = 0, old1 = 0, des0 = 0, des1 = 0;
+        if (pend0) {
+            if (__vcmpeq2(b0.x, pair0) | __vcmpeq2(b0.y, pair0) | __vcmpeq2(b0.z, pair0) | __vcmpeq2(b0.w, pair0)) {
+                *r0 = 1;
+                pend0 = false;
+            } else {
+                const uint32_t e0 = __vcmpeq2(b0.x, 0xFFFFFFFFu), e1 = __vcmpeq2(b0.y, 0xFFFFFFFFu);
+                const uint32_t e2 = __vcmpeq2(b0.z, 0xFFFFFFFFu), e3 = __vcmpeq2(b0.w, 0xFFFFFFFFu);
+                uint32_t e;
+                if (e0) { wi0 = 0; old0 = b0.x; e = e0; }
+                else if (e1) { wi0 = 1; old0 = b0.y; e = e1; }
+                else if (e2) { wi0 = 2; old0 = b0.z; e = e2; }
+                else if (e3) { wi0 = 3; old0 = b0.w; e = e3; }
+                else { e = 0; pend0 = false; }   // full: the bitset decides (r0 stays 2)
+                if (pend0) des0 = (e & 0xFFFFu) ? ((old0 & 0xFFFF0000u) | q0) : ((old0 & 0x0000FFFFu) | (q0 << 16));
+            }
+        }
+        if (pend1) {
+            if (__vcmpeq2(b1.x, pair1) | __vcmpeq2(b1.y, pair1) | __vcmpeq2(b1.z, pair1) | __vcmpeq2(b1.w, pair1)) {
+                *r1 = 1;
+                pend1 = false;
+            } else {
+                const uint32_t e0 = __vcmpeq2(b1.x, 0xFFFFFFFFu), e1 = __vcmpeq2(b1.y, 0xFFFFFFFFu);
+                const uint32_t e2 = __vcmpeq2(b1.z, 0xFFFFFFFFu), e3 = __vcmpeq2(b1.w, 0xFFFFFFFFu);
+                uint32_t e;
+                if (e0) { wi1 = 0; old1 = b1.x; e = e0; }
+                else if (e1) { wi1 = 1; old1 = b1.y; e = e1; }
+                else if (e2) { wi1 = 2; old1 = b1.z; e = e2; }
+                else if (e3) { wi1 = 3; old1 = b1.w; e = e3; }
+                else { e = 0; pend1 = false; }
+                if (pend1) des1 = (e & 0xFFFFu) ? ((old1 & 0xFFFF0000u) | q1) : ((old1 & 0x0000FFFFu) | (q1 << 16));
+            }
+        }
+        // A failed CAS means another insert filled that slot: read the bucket again.
+        if (pend0 && atomicCAS(reinterpret_cast<uint32_t*>(vs.tab + bk0) + wi0, old0, des0) == old0) {
+            *r0 = 0;
+            pend0 = false;
+        }
+        if (pend1 && atomicCAS(reinterpret_cast<uint32_t*>(vs.tab + bk1) + wi1, old1, des1) == old1) {
+            *r1 = 0;
+            pend1 = false;
+        }
+    }
+}
+
+// test_and_set for two ids per lane; all the ids of the warp are distinct.
+__device__ __forceinline__ void visited_test_and_set2(Visited& vs, uint32_t v0, bool a0, uint32_t v1, bool a1,
+                                                      bool* new0, bool* new1) {
+    const int lane = lane_id();
+    int t0 = a0 ? 2 : -1, t1 = a1 ? 2 : -1;
+    if (vs.tbits) table_test_insert2(vs, v0, a0, v1, a1, &t0, &t1);
+    bool n0 = t0 == 0, n1 = t1 == 0;
+    bool in0 = false, in1 = false;
+    if (t0 == 2) {
+        const uint32_t mask = 1u << (v0 & 31);
+        n0 = !(atomicOr(vs.bits + (v0 >> 5), mask) & mask);
+        in0 = n0;
+    }
+    if (t1 == 2) {
+        const uint32_t mask = 1u << (v1 & 31);
+        n1 = !(atomicOr(vs.bits + (v1 >> 5), mask) & mask);
+        in1 = n1;
+    }
+    const uint32_t b0 = __ballot_sync(kFull, in0), b1 = __ballot_sync(kFull, in1);
+    if (b0 | b1) {
+        const uint32_t lt = (1u << lane) - 1u;
+        const uint32_t pos0 = vs.list_n + __popc(b0 & lt);
+        const uint32_t pos1 = vs.list_n + __popc(b0) + __popc(b1 & lt);
+        if (in0 && pos0 < vs.list_cap) vs.list[pos0] = v0;
+        if (in1 && pos1 < vs.list_cap) vs.list[pos1] = v1;
+        const uint32_t total = vs.list_n + __popc(b0) + __popc(b1);
+        if (total > vs.list_cap) vs.list_overflow = true;
+        vs.list_n = min(total, vs.list_cap);
+        vs.global_used = true;
+    }
+    __syncwarp();
+    *new0 = n0;
+    *new1 = n1;
+}
+
 __device__ __forceinline__ void table_reset(const Visited& vs) {
     if (vs.tbits) {
         const uint32_t n = 1u << vs.tbits;
@@ -411,6 +501,26 @@ __device__ __forceinline__ void collect_unvisited(const DeviceGraph& g, Visited&
     __syncwarp();
     *cnt = c;
     *consumed = min(i, len);
+}
+
+// collect_unvisited for a whole level-0 row of at most 64 distinct ids,
+// preloaded as row[lane] (ids0) and row[32 + lane] (ids1), 0xffffffff past
+// len: one pass, two ids per lane. Ids are distinct, so the order in which
+// lanes insert them cannot change which are new; the new ones are written to
+// cvid in row order. Returns their count.
+__device__ __forceinline__ uint32_t collect_row64_unique(const DeviceGraph& g, Visited& vs, uint32_t ids0,
+                                                         uint32_t ids1, uint32_t len, uint32_t* cvid, int* error) {
+    const int lane = lane_id();
+    const bool in0 = static_cast<uint32_t>(lane) < len, in1 = static_cast<uint32_t>(lane) + 32u < len;
+    if ((in0 && ids0 >= g.n) || (in1 && ids1 >= g.n)) set_error(error, kErrBadVid);
+    bool n0, n1;
+    visited_test_and_set2(vs, ids0, in0 && ids0 < g.n, ids1, in1 && ids1 < g.n, &n0, &n1);
+    const uint32_t b0 = __ballot_sync(kFull, n0), b1 = __ballot_sync(kFull, n1);
+    const uint32_t lt = (1u << lane) - 1u;
+    if (n0) cvid[__popc(b0 & lt)] = ids0;
+    if (n1) cvid[__popc(b0) + __popc(b1 & lt)] = ids1;
+    __syncwarp();
+    return __popc(b0) + __popc(b1);
 }
 
 // ---------------------------------------------------------------------------
@@ -919,9 +1029,15 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
             ct.l0_row_ids += len;
             pc.lap(kPhPop);
             uint32_t pos = 0;
+            const bool one_pass = g.l0_unique && len <= 64u;
             while (pos < len) {
                 uint32_t cnt, consumed;
-                collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error, ids0, ids1, pos == 0);
+                if (one_pass) {
+                    cnt = collect_row64_unique(g, vs, ids0, ids1, len, cvid, a.error);
+                    consumed = len;
+                } else {
+                    collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error, ids0, ids1, pos == 0);
+                }
                 pos = consumed;
                 pc.lap(kPhCollect);
                 if (cnt == 0) continue;

@@ -151,6 +151,7 @@ int launch_serving(artea_gpu_server* s) {
     a.g.dim = ix->dim;
     a.g.top = ix->top;
     a.g.entry = ix->entry;
+    a.g.l0_unique = ix->l0_unique;
     for (int h = 0; h < kMaxGroups; ++h) a.g.offsets[h] = ix->group_ptr[h];
     a.queries = s->d_q;
     a.nq = s->ring;
