@@ -6,7 +6,8 @@ the reference's CPU builder) and its FP32 vectors are uploaded once; queries
 run in hand-written CUDA kernels behind the C-ABI of include/artea_gpu.h.
 """
 from .graph import CompactHierarchicalGraph  # noqa: F401
-from .router import DeviceIndex, GpuRouter, HierarchicalGraphRouter, entry_dists, entry_vids  # noqa: F401
+from .router import (BruteforceRouter, DeviceIndex, GpuRouter, HierarchicalGraphRouter, entry_dists,  # noqa: F401
+                     entry_vids)
 
-__all__ = ["CompactHierarchicalGraph", "DeviceIndex", "GpuRouter", "HierarchicalGraphRouter", "entry_vids",
-           "entry_dists"]
+__all__ = ["BruteforceRouter", "CompactHierarchicalGraph", "DeviceIndex", "GpuRouter", "HierarchicalGraphRouter",
+           "entry_vids", "entry_dists"]

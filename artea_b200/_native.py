@@ -118,6 +118,10 @@ SIGNATURES = {
     "artea_gpu_router_launches": (c_int, [c_void_p, POINTER(c_uint64)]),
     "artea_gpu_router_set_phase_buffer": (c_int, [c_void_p, c_void_p]),
     "artea_gpu_router_set_early_stop": (c_int, [c_void_p, c_void_p, c_uint32]),
+    "artea_gpu_bruteforce": (c_int, [c_void_p, c_int, c_void_p, c_uint32, c_uint32, c_void_p, c_uint32, c_void_p]),
+    "artea_gpu_centroid_entry": (c_int, [c_void_p, c_int, c_void_p, c_uint32, c_void_p]),
+    "artea_gpu_bruteforce_device": (c_int, [c_void_p, c_int, c_void_p, c_uint32, c_uint32, c_void_p, c_uint32,
+                                            c_void_p, c_void_p]),
     "artea_gpu_server_create": (c_int, [c_void_p, POINTER(ServerOpts), POINTER(c_void_p)]),
     "artea_gpu_server_submit": (c_int, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, POINTER(c_uint64)]),
     "artea_gpu_server_poll": (c_int, [c_void_p, c_uint64, c_uint32, c_uint32, c_void_p, POINTER(c_int)]),

@@ -511,6 +511,7 @@ int artea_gpu_index_create(const artea_gpu_graph_desc* g, const float* vectors, 
     ix->device = device;
     ix->n = g->num_vertices;
     ix->dim = dim;
+    ix->nvecs = num_vectors;
     const bool empty = g->num_vertices == 0 || g->top_level == kInvalidLevel;
     ix->top = empty ? kInvalidLevel : g->top_level;
     ix->entry = g->entry_point_vid;

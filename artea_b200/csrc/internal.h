@@ -24,6 +24,7 @@ struct artea_gpu_index {
     int device = 0;
     uint32_t n = 0, dim = 0, top = artea_gpu::kInvalidLevel, entry = 0, ul = 0, bl = 0;
     uint32_t l0_unique = 0;   // level-0 rows of <= 64 ids hold distinct ids (checked at upload)
+    uint32_t nvecs = 0;       // vector rows uploaded (brute force scans all of them)
     float* d_vecs = nullptr;
     uint2* d_vinfo = nullptr;
     uint32_t* d_nbrs = nullptr;

@@ -95,6 +95,32 @@ class DeviceIndex:
         nat.check(nat.lib().artea_gpu_index_bytes(self.handle, ctypes.byref(b)))
         return int(b.value)
 
+    def bruteforce(self, queries: np.ndarray, topk: int, metric, subset: Optional[np.ndarray] = None) -> np.ndarray:
+        """Exact brute-force top-k over this index's vectors (artea_gpu_bruteforce):
+        (nq, topk) CandidateEntry words, ascending, CandidateEntry() padding."""
+        q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, self.dim)
+        sub = None if subset is None else np.ascontiguousarray(subset, dtype=np.uint32)
+        out = np.empty((q.shape[0], topk), dtype=np.uint64)
+        nat.check(nat.lib().artea_gpu_bruteforce(self.handle, metric_code(metric), nat.ptr(q), q.shape[0], topk,
+                                                 nat.ptr(sub), 0 if sub is None else sub.size, nat.ptr(out)))
+        return out
+
+    def centroid_entry(self, metric, bucket: Optional[np.ndarray] = None) -> int:
+        """The compactor's entry point: the bucket vid nearest to the bucket's
+        centroid (artea_gpu_centroid_entry); 0xFFFFFFFF for an empty bucket."""
+        b = None if bucket is None else np.ascontiguousarray(bucket, dtype=np.uint32)
+        out = ctypes.c_uint32()
+        nat.check(nat.lib().artea_gpu_centroid_entry(self.handle, metric_code(metric), nat.ptr(b),
+                                                     0 if b is None else b.size, ctypes.byref(out)))
+        return int(out.value)
+
+    def bruteforce_device(self, d_queries, nq: int, topk: int, metric, d_out, d_subset=None, n_subset: int = 0,
+                          stream: int = 0) -> None:
+        """artea_gpu_bruteforce_device on device buffers (torch tensors or addresses)."""
+        nat.check(nat.lib().artea_gpu_bruteforce_device(self.handle, metric_code(metric), nat.ptr(d_queries), nq,
+                                                        topk, nat.ptr(d_subset), n_subset, nat.ptr(d_out),
+                                                        ctypes.c_void_p(stream or None)))
+
     def close(self) -> None:
         if getattr(self, "_h", None) is not None:
             nat.lib().artea_gpu_index_destroy(self._h)
@@ -105,6 +131,50 @@ class DeviceIndex:
             self.close()
         except Exception:
             pass
+
+
+def vectors_only_graph() -> CompactHierarchicalGraph:
+    """An empty compact graph: a DeviceIndex over it holds vectors only."""
+    return CompactHierarchicalGraph(0, 0, 4, 4, 0xFFFFFFFF, np.zeros((0, 2), np.uint32), [np.zeros(1, np.uint64)],
+                                    np.zeros(0, np.uint32))
+
+
+class BruteforceRouter:
+    """Drop-in for bruteforce_router_t<Metric, Dim> (router/bruteforce_router.hpp):
+    exact k-NN over base_vecs on the GPU, distances bit-identical to the
+    reference's; equal distances come in vid order."""
+
+    def __init__(self, base_vecs: np.ndarray, metric, topk: int, device: int = 0):
+        self.base_vecs = base_vecs
+        self.metric = metric_code(metric)
+        self.topk = int(topk)
+        self.device = device
+        self._index = None
+
+    def initialize(self) -> None:
+        """bruteforce_router.hpp:63-65 (nothing to prepare); the vectors are uploaded on first use."""
+        nat.lib()
+
+    def _ix(self) -> DeviceIndex:
+        if self._index is None:
+            self._index = DeviceIndex(vectors_only_graph(), self.base_vecs, self.device)
+        return self._index
+
+    def query(self, query_vec: np.ndarray, subset: Optional[np.ndarray] = None) -> np.ndarray:
+        """query (:74-96) / query with subset (:100-125): min(topk, candidates) words."""
+        n = self._ix().num_vectors if subset is None else len(subset)
+        words = self._ix().bruteforce(np.asarray(query_vec, dtype=np.float32).reshape(1, -1), self.topk,
+                                      self.metric, subset)[0]
+        return words[: min(self.topk, n)]
+
+    def batch_query(self, query_vecs: np.ndarray, subset: Optional[np.ndarray] = None) -> np.ndarray:
+        """batch_query (:130-160, subset :164-190): (nq * topk,) words, CandidateEntry() padding."""
+        return self._ix().bruteforce(query_vecs, self.topk, self.metric, subset).reshape(-1)
+
+    def close(self) -> None:
+        if self._index is not None:
+            self._index.close()
+            self._index = None
 
 
 class GpuRouter:

@@ -122,43 +122,19 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# Ground truth (exact top-k by distance, ties by vid), on the GPU with torch.
+# Ground truth: the exact brute-force top-k of the search metric (the
+# reference's bruteforce_router_t semantics, distances bit-identical), computed
+# by artea_gpu_bruteforce on the uploaded index; equal distances in vid order.
 # ---------------------------------------------------------------------------
-def ground_truth(base: np.ndarray, queries: np.ndarray, k: int, metric: str, device, cache_dir: str) -> np.ndarray:
-    import torch
-    path = os.path.join(cache_dir, f"gt-{metric}-{k}-{ds.fingerprint(base)}-{ds.fingerprint(queries)}.npy")
+def ground_truth(index, base: np.ndarray, queries: np.ndarray, k: int, metric: str, cache_dir: str) -> np.ndarray:
+    path = os.path.join(cache_dir, f"gtbf-{metric}-{k}-{ds.fingerprint(base)}-{ds.fingerprint(queries)}.npy")
     if os.path.exists(path):
         return np.load(path)
-    torch.backends.cuda.matmul.allow_tf32 = False
-    xb = torch.from_numpy(base).to(device)
-    xb64 = xb.double()
-    xn = (xb * xb).sum(1)
     out = np.empty((queries.shape[0], k), dtype=np.uint32)
-    extra = 64
-    for lo in range(0, queries.shape[0], 256):
-        q = torch.from_numpy(queries[lo:lo + 256]).to(device)
-        if metric == "euclidean":
-            d = (q * q).sum(1, keepdim=True) - 2.0 * (q @ xb.T) + xn[None, :]
-        elif metric == "cosine":
-            d = 1.0 - (q @ xb.T) / (q.norm(dim=1, keepdim=True) * xb.norm(dim=1)[None, :]).clamp_min(1e-30)
-        else:
-            d = -(q @ xb.T)
-        cand = torch.topk(d, min(k + extra, d.shape[1]), dim=1, largest=False).indices
-        q64 = q.double()[:, None, :]
-        rows = xb64[cand]
-        if metric == "euclidean":
-            ex = ((rows - q64) ** 2).sum(-1)
-        elif metric == "cosine":
-            ex = 1.0 - (rows * q64).sum(-1) / (rows.norm(dim=-1) * q64.norm(dim=-1)).clamp_min(1e-300)
-        else:
-            ex = -(rows * q64).sum(-1)
-        # sort by (distance, vid)
-        order = torch.argsort(cand, dim=1)
-        cand = torch.gather(cand, 1, order)
-        ex = torch.gather(ex, 1, order)
-        order = torch.argsort(ex, dim=1, stable=True)
-        out[lo:lo + 256] = torch.gather(cand, 1, order)[:, :k].cpu().numpy().astype(np.uint32)
-    del xb, xb64
+    for lo in range(0, queries.shape[0], 2048):
+        words = index.bruteforce(queries[lo:lo + 2048], k, metric_code(metric))
+        out[lo:lo + 2048] = (words & np.uint64(0x7FFFFFFF)).astype(np.uint32)
+    os.makedirs(cache_dir, exist_ok=True)
     np.save(path, out)
     return out
 
@@ -294,7 +270,7 @@ def run_uneven(args, w, base, queries, hgra, report, index, device, metric, cach
     nq, dim = queries.shape
     topk, queue = ds.per_query_params(w, nq)
     kmax = int(topk.max())
-    gt = ground_truth(base, queries, kmax, w.metric, device, cache_dir)
+    gt = ground_truth(index, base, queries, kmax, w.metric, cache_dir)
     d_q = torch.from_numpy(queries).to(device)
     d_tk = torch.from_numpy(topk.view(np.int32)).to(device)
     d_qu = torch.from_numpy(queue.view(np.int32)).to(device)
@@ -391,7 +367,7 @@ def run_serving(args, w, base, queries, report, index, device, metric, cache_dir
     from artea_b200.serving import Server, make_requests, run_per_batch, run_poisson
     nq = min(args.serve_queries, queries.shape[0])
     qs = queries[:nq]
-    gt = ground_truth(base, queries, 100, w.metric, device, cache_dir)[:nq]
+    gt = ground_truth(index, base, queries, 100, w.metric, cache_dir)[:nq]
     rates = [float(x) for x in args.serve_rates.split(",") if x]
     srv = Server(index, metric, max_topk=100, max_queue=400, ring_slots=16384, mode=args.mode)
     points = []
@@ -531,7 +507,7 @@ def main() -> None:
         run_uneven(args, w, base, queries, hgra, report, index, device, metric, cache_dir, rank, world)
         index.close()
         return
-    gt = ground_truth(base, queries, k, w.metric, device, cache_dir) if rank == 0 else None
+    gt = ground_truth(index, base, queries, k, w.metric, cache_dir) if rank == 0 else None
 
     d_q = torch.from_numpy(queries).to(device)
     d_out = torch.empty((nq, k), dtype=torch.int64, device=device)

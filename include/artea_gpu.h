@@ -226,6 +226,36 @@ int artea_gpu_router_launches(const artea_gpu_router* router, uint64_t* launches
  * no thresholds (any array is accepted). */
 int artea_gpu_router_set_early_stop(artea_gpu_router* router, const float* level_thresholds, uint32_t n_levels);
 
+/* Exact brute-force k-NN over the index's vectors: BruteforceRouter::batch_query
+ * (router/bruteforce_router.hpp:130-160) and, with a subset, the subset
+ * overload (:164-190, ids are original vector ids). out gets nq rows of topk
+ * CandidateEntry words: the min(topk, candidates) nearest in ascending
+ * distance (the reference's partial_sort leaves the order of equal distances
+ * unspecified; here they come in vid order), then CandidateEntry() padding
+ * (vid 0xFFFFFFFF, distance 0). Distances are bit-identical to the reference's
+ * SIMD functor. The index may have an empty graph (only its vectors are read).
+ * topk in [1, 1024]. subset NULL = all vectors; a non-NULL subset with
+ * n_subset 0 gives padding only. The host variant checks subset ids against
+ * the vector count (EINVAL) and waits for the result. */
+int artea_gpu_bruteforce(const artea_gpu_index* index, int metric, const float* queries, uint32_t nq, uint32_t topk,
+                         const uint32_t* subset, uint32_t n_subset, uint64_t* out);
+
+/* The same on device buffers (d_subset ids must be < the vector count); runs on
+ * stream (NULL = the default stream) and waits for it before returning. */
+int artea_gpu_bruteforce_device(const artea_gpu_index* index, int metric, const float* d_queries, uint32_t nq,
+                                uint32_t topk, const uint32_t* d_subset, uint32_t n_subset, uint64_t* d_out,
+                                void* stream);
+
+/* The compactor's entry point (hierarchical_graph_compactor.hpp:261-327,
+ * _compute_entry_point_vid): the centroid of bucket's vectors (double sums,
+ * rounded to float), then the bucket vid nearest to it under metric (the
+ * build metric: EUCLIDEAN for L2 graphs). bucket NULL = all vectors; an empty
+ * bucket gives 0xFFFFFFFF (invalid_vertex_id). Equal distances resolve to the
+ * smallest vid (the reference's parallel reduce leaves them open). EINVAL for
+ * ids out of range. Waits for the result. */
+int artea_gpu_centroid_entry(const artea_gpu_index* index, int metric, const uint32_t* bucket, uint32_t n,
+                             uint32_t* out_vid);
+
 /* Profiling hook: when d_phase_cycles (device memory, nq x 8 uint64) is set,
  * every later launch writes per-query SM clock cycles spent in: greedy upper
  * levels, pop/row lookup, row ids + visited, distances, queue merge, tail,

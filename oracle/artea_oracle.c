@@ -407,6 +407,32 @@ int oracle_batch_query_early_stop(const oracle_graph* g, const float* vecs, uint
     return run_batch(g, vecs, dim, queries, nq, topk, queue, k_stride, metric, 0, out, stats, threads, thr);
 }
 
+/* _compute_entry_point_vid (index/compactor/hierarchical_graph_compactor.hpp:
+ * 261-327): double per-dimension sums over the bucket, centroid rounded to
+ * float, then the bucket vid with the smallest distance to it (ties: first in
+ * bucket order). bucket NULL = [0, n). Returns 0xFFFFFFFF for an empty bucket. */
+uint32_t oracle_centroid_entry(const float* vecs, uint32_t dim, const uint32_t* bucket, uint32_t n, int metric) {
+    if (n == 0) return 0xFFFFFFFFu;
+    double* sums = (double*)calloc(dim, sizeof(double));
+    float* c = (float*)malloc(sizeof(float) * dim);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* v = vecs + (size_t)(bucket ? bucket[i] : i) * dim;
+        for (uint32_t d = 0; d < dim; ++d) sums[d] += (double)v[d];
+    }
+    const double inv = 1.0 / (double)n;
+    for (uint32_t d = 0; d < dim; ++d) c[d] = (float)(sums[d] * inv);
+    float best = FLT_MAX;
+    uint32_t best_vid = 0xFFFFFFFFu;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t vid = bucket ? bucket[i] : i;
+        const float dd = oracle_distance(metric, c, vecs + (size_t)vid * dim, dim);
+        if (dd < best) { best = dd; best_vid = vid; }
+    }
+    free(sums);
+    free(c);
+    return best_vid;
+}
+
 /* ---------------------------------------------------------------------------
  * Exact top-k (router/bruteforce_router.hpp:74-160 idea: full scan + partial
  * sort), ties broken by vid.

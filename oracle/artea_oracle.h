@@ -79,6 +79,10 @@ int oracle_batch_query_early_stop(const oracle_graph* g, const float* vecs, uint
                                   int metric, const float* cfg_thresholds, uint32_t n_levels,
                                   uint64_t* out, oracle_stats* stats, int threads);
 
+/* The compactor's centroid entry point (hierarchical_graph_compactor.hpp:261-327):
+ * bucket NULL = vectors [0, n); 0xFFFFFFFF for an empty bucket. */
+uint32_t oracle_centroid_entry(const float* vecs, uint32_t dim, const uint32_t* bucket, uint32_t n, int metric);
+
 /* Exact top-k by (distance, vid) over all vectors: ground truth. */
 int oracle_bruteforce(const float* vecs, uint32_t n, uint32_t dim, const float* queries, uint32_t nq,
                       uint32_t k, int metric, uint32_t* out_ids, float* out_dists, int threads);

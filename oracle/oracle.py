@@ -57,6 +57,8 @@ def oracle_lib():
         L.oracle_batch_query_early_stop.argtypes = [POINTER(_Graph), c_void_p, c_uint32, c_void_p, c_uint32, c_void_p,
                                                     c_void_p, c_uint32, c_int, c_void_p, c_uint32, c_void_p, c_void_p,
                                                     c_int]
+        L.oracle_centroid_entry.restype = c_uint32
+        L.oracle_centroid_entry.argtypes = [c_void_p, c_uint32, c_void_p, c_uint32, c_int]
         L.oracle_bruteforce.restype = c_int
         L.oracle_bruteforce.argtypes = [c_void_p, c_uint32, c_uint32, c_void_p, c_uint32, c_uint32, c_int, c_void_p,
                                         c_void_p, c_int]
@@ -84,6 +86,9 @@ def ref_lib():
         L.artea_ref_batch_query_early_stop.restype = c_int
         L.artea_ref_batch_query_early_stop.argtypes = [c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_int,
                                                        c_void_p, c_uint32, c_void_p, c_void_p]
+        L.artea_ref_bruteforce.restype = c_int
+        L.artea_ref_bruteforce.argtypes = [c_void_p, c_void_p, c_uint32, c_uint32, c_int, c_void_p, c_uint32,
+                                           c_void_p]
         L.artea_ref_distance.restype = c_float
         L.artea_ref_distance.argtypes = [c_int, c_void_p, c_void_p, c_uint32]
         L.artea_ref_max_threads.restype = c_int
@@ -165,6 +170,14 @@ def bruteforce(base: np.ndarray, queries: np.ndarray, k: int, metric: int = 0, t
     return ids, d
 
 
+def centroid_entry(base: np.ndarray, metric: int, bucket=None) -> int:
+    """C restatement of the compactor's centroid entry point."""
+    base = np.ascontiguousarray(base, dtype=np.float32)
+    b = None if bucket is None else np.ascontiguousarray(bucket, dtype=np.uint32)
+    n = base.shape[0] if b is None else b.size
+    return int(oracle_lib().oracle_centroid_entry(_p(base), base.shape[1], _p(b), n, metric))
+
+
 class RefRouter:
     """The reference's hierarchical_graph_router_t over an HGRA snapshot."""
 
@@ -203,6 +216,18 @@ class RefRouter:
         if rc != 0:
             raise RuntimeError(ref_lib().artea_ref_last_error().decode())
         return (out, calls) if count_distances else out
+
+    def bruteforce(self, queries: np.ndarray, topk: int, metric: int = 0, subset=None) -> np.ndarray:
+        """The reference's bruteforce_router_t batch_query (with subset: the subset
+        overload): (nq, topk) words, CandidateEntry() padding."""
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        sub = None if subset is None else np.ascontiguousarray(subset, dtype=np.uint32)
+        out = np.empty((q.shape[0], topk), dtype=np.uint64)
+        rc = ref_lib().artea_ref_bruteforce(self._h, _p(q), q.shape[0], topk, metric, _p(sub),
+                                            0 if sub is None else sub.size, _p(out))
+        if rc != 0:
+            raise RuntimeError(ref_lib().artea_ref_last_error().decode())
+        return out
 
     def close(self):
         if self._h:

@@ -156,9 +156,38 @@ int by_dim(RefIndex& idx, const float* q, uint32_t nq, uint32_t k, uint32_t L, i
     throw std::invalid_argument("unsupported padded dim " + std::to_string(idx.vecs.get_vec_dim()));
 }
 
+// bruteforce_router_t<Metric, Dim>::batch_query (router/bruteforce_router.hpp:130-160)
+// or, with subset != null, its subset overload (:164-190). out: nq*topk words.
+template <DistanceMetricsT Metric, vec_dim_t Dim>
+int run_bruteforce(RefIndex& idx, const float* queries, uint32_t nq, uint32_t topk, const uint32_t* subset,
+                   uint32_t n_subset, uint64_t* out) {
+    vector_array_t qv = copy_rows(queries, nq, Dim);
+    dist_func_t<Metric, Dim> dist;
+    bruteforce_router_t<Metric, Dim> router(idx.vecs, dist, topk);
+    router.initialize();
+    const auto res = subset ? router.batch_query(qv, std::span<const uint32_t>(subset, n_subset))
+                            : router.batch_query(qv);
+    std::memcpy(out, res.data(), sizeof(uint64_t) * res.size());
+    return 0;
+}
+
+template <DistanceMetricsT Metric>
+int by_dim_bf(RefIndex& idx, const float* q, uint32_t nq, uint32_t k, const uint32_t* s, uint32_t ns,
+              uint64_t* out) {
+    switch (idx.vecs.get_vec_dim()) {
+        case 16: return run_bruteforce<Metric, 16>(idx, q, nq, k, s, ns, out);
+        case 96: return run_bruteforce<Metric, 96>(idx, q, nq, k, s, ns, out);
+        case 128: return run_bruteforce<Metric, 128>(idx, q, nq, k, s, ns, out);
+        case 960: return run_bruteforce<Metric, 960>(idx, q, nq, k, s, ns, out);
+        default: break;
+    }
+    throw std::invalid_argument("unsupported padded dim " + std::to_string(idx.vecs.get_vec_dim()));
+}
+
 }  // namespace
 
 extern "C" {
+
 
 const char* artea_ref_last_error() { return g_last_error.c_str(); }
 
@@ -217,6 +246,23 @@ int artea_ref_batch_query_early_stop(void* h, const float* queries, uint32_t nq,
     } catch (const std::overflow_error& e) {
         g_last_error = e.what();
         return -2;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+int artea_ref_bruteforce(void* h, const float* queries, uint32_t nq, uint32_t topk, int metric,
+                                    const uint32_t* subset, uint32_t n_subset, uint64_t* out) {
+    try {
+        auto& idx = *static_cast<RefIndex*>(h);
+        switch (metric) {
+            case 0: return by_dim_bf<DistanceMetricsT::EUCLIDEAN_SQR>(idx, queries, nq, topk, subset, n_subset, out);
+            case 1: return by_dim_bf<DistanceMetricsT::EUCLIDEAN>(idx, queries, nq, topk, subset, n_subset, out);
+            case 2: return by_dim_bf<DistanceMetricsT::COSINE>(idx, queries, nq, topk, subset, n_subset, out);
+            case 3: return by_dim_bf<DistanceMetricsT::DOT>(idx, queries, nq, topk, subset, n_subset, out);
+            default: throw std::invalid_argument("unknown metric");
+        }
     } catch (const std::exception& e) {
         g_last_error = e.what();
         return -1;

@@ -81,3 +81,25 @@ def gpu_available():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def assert_same_knn(got: np.ndarray, want: np.ndarray, what: str = "") -> None:
+    """Rows of CandidateEntry words that must agree except for the order of
+    entries at equal distance (the reference's partial_sort leaves it open):
+    identical distance bits position by position, identical id sets per
+    distance value, identical words everywhere else."""
+    assert got.shape == want.shape, (got.shape, want.shape, what)
+    gd = (got >> np.uint64(32)).astype(np.uint32)
+    wd = (want >> np.uint64(32)).astype(np.uint32)
+    np.testing.assert_array_equal(gd, wd, err_msg=f"{what}: distances")
+    for i in range(got.shape[0]):
+        if np.array_equal(got[i], want[i]):
+            continue
+        for dv in np.unique(wd[i]):
+            g = np.sort(got[i][gd[i] == dv] & np.uint64(0xFFFFFFFF))
+            w = np.sort(want[i][wd[i] == dv] & np.uint64(0xFFFFFFFF))
+            if np.array_equal(g, w):
+                continue
+            # A tie group cut by the k boundary may hold different members.
+            at_end = gd[i][-1] == dv
+            assert at_end and g.size == w.size, f"{what}: row {i} ids differ at distance bits {dv:#x}"

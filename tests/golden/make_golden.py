@@ -196,7 +196,43 @@ def early_stop_fixtures() -> None:
         add_early_stop(name, [[0.0] + [entry_threshold(path, q)] * top for q in (0.2, 0.5)])
 
 
+def add_bruteforce(name: str, topks, subset_seed: int = 5) -> None:
+    """Adds the reference bruteforce_router_t's batch_query words for each topk
+    (bf_k{k}) and, over a seeded subset of the vectors, its subset overload
+    (bf_subset, bf_sub_k{k})."""
+    path = os.path.join(HERE, f"{name}.npz")
+    d = dict(np.load(path))
+    for key in [k for k in d if k.startswith("bf_")]:
+        del d[key]
+    base = d["base"].astype(np.float32)
+    rng = np.random.default_rng(subset_seed)
+    subset = np.sort(rng.choice(base.shape[0], size=max(1, base.shape[0] // 3), replace=False)).astype(np.uint32)
+    with tempfile.TemporaryDirectory() as tmp:
+        hgra = os.path.join(tmp, "g.hgra")
+        with open(hgra, "wb") as f:
+            f.write(d["hgra"].tobytes())
+        r = orc.RefRouter(hgra, base)
+        d["bf_subset"] = subset
+        for k in topks:
+            d[f"bf_k{k}"] = r.bruteforce(d["queries"], k, metric=int(d["metric"]))
+            d[f"bf_sub_k{k}"] = r.bruteforce(d["queries"], k, metric=int(d["metric"]), subset=subset)
+        r.close()
+    np.savez_compressed(path, **d)
+    print(name, "bruteforce:", list(topks))
+
+
+def bruteforce_fixtures() -> None:
+    add_bruteforce("early_stop_top2", [1, 3, 10])      # 4 vectors: topk 10 pads
+    add_bruteforce("axis80", [10, 100])                 # tied distances
+    add_bruteforce("sift2k", [10, 100])
+    add_bruteforce("deep1k_cos", [10, 64])
+    add_bruteforce("gist400", [10, 50])
+
+
 def main() -> None:
+    if "--bruteforce-only" in sys.argv:
+        bruteforce_fixtures()
+        return
     if "--early-stop-only" in sys.argv:
         early_stop_fixtures()
         return
@@ -212,6 +248,7 @@ def main() -> None:
     built_case("deep1k_cos", "deep10m", 1000, 48, "cosine", 2, 10, [16, 64])
     built_case("gist400", "gist1m", 400, 24, "euclidean", 0, 10, [20, 50], l0=0.05)
     early_stop_fixtures()
+    bruteforce_fixtures()
 
 
 if __name__ == "__main__":

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from conftest import EARLY_STOP_CASES, GOLDEN_CASES, golden_case
+from conftest import EARLY_STOP_CASES, GOLDEN_CASES, assert_same_knn, golden_case
 from oracle import oracle as orc
 
 
@@ -191,3 +191,36 @@ def test_early_stop_thresholds_shorter_than_the_hierarchy_are_rejected():
     c = golden_case("early_stop_top2")
     with pytest.raises(ValueError):
         orc.batch_query(c.graph, c.base, c.queries, 1, 4, metric=1, early_stop=[0, 8])
+
+
+BRUTEFORCE_CASES = [("early_stop_top2", [1, 3, 10]), ("axis80", [10, 100]), ("sift2k", [10, 100]),
+                    ("deep1k_cos", [10, 64]), ("gist400", [10, 50])]
+
+
+@pytest.mark.parametrize("name,topks", BRUTEFORCE_CASES)
+def test_oracle_bruteforce_matches_reference_bruteforce_router(name, topks):
+    # bruteforce_router.hpp:74-160: exact distances; equal distances may come in
+    # any order in the reference (partial_sort), in vid order in the oracle.
+    import numpy as _np
+    z = _np.load(f"{__import__('conftest').GOLDEN}/{name}.npz")
+    c = golden_case(name)
+    for k in topks:
+        want = z[f"bf_k{k}"]
+        ids, d = orc.bruteforce(c.base, c.queries, k, metric=c.metric, threads=4)
+        keff = min(k, c.base.shape[0])
+        words = (d.view(_np.uint32).astype(_np.uint64) << _np.uint64(32)) | ids.astype(_np.uint64)
+        assert_same_knn(words[:, :keff], want[:, :keff], f"{name} k={k}")
+        # the reference pads with CandidateEntry(): vid all ones, distance 0
+        assert (want[:, keff:] == _np.uint64(0xFFFFFFFF)).all()
+
+
+@pytest.mark.parametrize("name,metric", [("sift2k", 1), ("deep1k_cos", 2), ("gist400", 1)])
+def test_oracle_centroid_entry_matches_the_reference_compactor(name, metric):
+    # hierarchical_graph_compactor.hpp:236-248: the compacted graph's entry
+    # point is the top bucket's vid nearest its centroid, under the build
+    # metric (true L2 for the Euclidean graphs).
+    c = golden_case(name)
+    top = c.graph.top_occupied_level_id()
+    bucket = np.nonzero(c.graph.vertex_info[:, 0] == top)[0].astype(np.uint32)
+    assert orc.centroid_entry(c.base, metric, bucket) == c.graph.entry_point_vid
+    assert orc.centroid_entry(c.base, metric, np.zeros(0, np.uint32)) == 0xFFFFFFFF
