@@ -78,6 +78,7 @@ class RouterOpts(ctypes.Structure):
         ("use_graphs", c_uint32),
         ("visited_hash_bits", c_uint32),
         ("register_budget", c_uint32),
+        ("stage_rows", c_uint32),
     ]
 
 
@@ -129,7 +130,8 @@ SIGNATURES = {
     "artea_gpu_server_destroy": (c_int, [c_void_p]),
     "artea_gpu_batch_query_noalloc": (c_int, [c_void_p, c_int, c_int, c_uint32, c_uint32, c_void_p, c_uint32, c_uint32,
                                               c_void_p, c_void_p]),
-    "artea_gpu_router_tuning": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32)]),
+    "artea_gpu_router_tuning": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32),
+                                        POINTER(c_uint32)]),
 }
 
 

@@ -44,6 +44,7 @@ struct Tuning {
     uint32_t warps = 4;
     uint32_t vh_bits = 11;
     uint32_t regs = 0;   // 0: 85-register budget, 1: 64-register budget
+    uint32_t stage = 0;  // 0: rows read with vector loads; kStageRows: TMA-staged in shared memory
 };
 
 // Identity of a captured launch: the buffers, sizes and launch parameters.
@@ -63,7 +64,7 @@ struct artea_gpu_router {
     artea_gpu_index* idx = nullptr;
     uint32_t topk = 0, queue = 0, max_queue = 0, cap = 0, max_batch = 0;
     int metric = 0, mode = 0, schedule = 0;
-    uint32_t want_warps = 0, want_ctas_per_sm = 0, want_vh_bits = 0, want_regs = 0;
+    uint32_t want_warps = 0, want_ctas_per_sm = 0, want_vh_bits = 0, want_regs = 0, want_stage = 0;
     bool use_graphs = false;
     cudaStream_t stream = nullptr;
     int num_sms = 0;
@@ -135,32 +136,39 @@ using namespace artea_gpu;
 // Router option visited_hash_bits: 0 = autotuned, ~0u = no hash, else log2 size.
 constexpr uint32_t kNoHash = 0xffffffffu;
 uint32_t hash_bits_of(uint32_t want) { return want == kNoHash ? 0u : want; }
+// Router option stage_rows: 0 = autotuned, ~0u = vector loads, else staged.
+uint32_t stage_of(uint32_t want) { return want == kNoHash ? 0u : kStageRows; }
 
 using KernelFn = void (*)(SearchArgs);
 
-// regs: 0 = 85-register budget, 1 = 64-register budget (persistent only).
+// regs: 0 = 85-register budget, 1 = 64-register budget (persistent only);
+// stage: rows staged in shared memory by TMA (persistent only).
+template <int kMetric, bool kExact>
+KernelFn pick_persistent(uint32_t regs, bool stage) {
+    if (stage)
+        return regs == 1 ? search_persistent_kernel<kMetric, kExact, 4, true>
+                         : search_persistent_kernel<kMetric, kExact, 3, true>;
+    return regs == 1 ? search_persistent_kernel<kMetric, kExact, 4> : search_persistent_kernel<kMetric, kExact, 3>;
+}
+
 template <int kMetric>
-KernelFn pick_kernel_m(bool exact, bool persistent, uint32_t regs) {
-    if (persistent) {
-        if (regs == 1)
-            return exact ? search_persistent_kernel<kMetric, true, 4> : search_persistent_kernel<kMetric, false, 4>;
-        return exact ? search_persistent_kernel<kMetric, true, 3> : search_persistent_kernel<kMetric, false, 3>;
-    }
+KernelFn pick_kernel_m(bool exact, bool persistent, uint32_t regs, bool stage) {
+    if (persistent) return exact ? pick_persistent<kMetric, true>(regs, stage) : pick_persistent<kMetric, false>(regs, stage);
     return exact ? search_plain_kernel<kMetric, true> : search_plain_kernel<kMetric, false>;
 }
 
-KernelFn pick_kernel(int metric, bool exact, bool persistent, uint32_t regs = 0) {
+KernelFn pick_kernel(int metric, bool exact, bool persistent, uint32_t regs = 0, bool stage = false) {
     switch (metric) {
-        case ARTEA_GPU_EUCLIDEAN_SQR: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN_SQR>(exact, persistent, regs);
-        case ARTEA_GPU_EUCLIDEAN: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN>(exact, persistent, regs);
-        case ARTEA_GPU_COSINE: return pick_kernel_m<ARTEA_GPU_COSINE>(exact, persistent, regs);
-        case ARTEA_GPU_DOT: return pick_kernel_m<ARTEA_GPU_DOT>(exact, persistent, regs);
+        case ARTEA_GPU_EUCLIDEAN_SQR: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN_SQR>(exact, persistent, regs, stage);
+        case ARTEA_GPU_EUCLIDEAN: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN>(exact, persistent, regs, stage);
+        case ARTEA_GPU_COSINE: return pick_kernel_m<ARTEA_GPU_COSINE>(exact, persistent, regs, stage);
+        case ARTEA_GPU_DOT: return pick_kernel_m<ARTEA_GPU_DOT>(exact, persistent, regs, stage);
         default: return nullptr;
     }
 }
 
-uint32_t smem_bytes_per_warp(uint32_t dim, uint32_t cap, uint32_t vh_bits) {
-    return warp_smem_words(dim, cap, vh_bits) * 4u;
+uint32_t smem_bytes_per_warp(uint32_t dim, uint32_t cap, uint32_t vh_bits, uint32_t stage = 0) {
+    return warp_smem_words(dim, cap, vh_bits, stage) * 4u;
 }
 
 // Captured graphs hold buffer addresses: drop them whenever a buffer moves.
@@ -210,14 +218,15 @@ int ensure_stage(artea_gpu_router* r, uint32_t nq, uint32_t k_stride) {
 
 // Persistent grid for a tuning point: as many CTAs per SM as fit.
 int persistent_shape(artea_gpu_router* r, const Tuning& t, LaunchShape* s) {
-    const uint64_t key = (static_cast<uint64_t>(t.warps) << 32) | (t.vh_bits << 1) | t.regs;
+    const uint64_t key = (static_cast<uint64_t>(t.warps) << 32) | (static_cast<uint64_t>(t.stage) << 16) |
+                         (t.vh_bits << 1) | t.regs;
     auto hit = r->shapes.find(key);
     if (hit != r->shapes.end()) {
         *s = hit->second;
         return ARTEA_GPU_OK;
     }
-    KernelFn fn = pick_kernel(r->metric, r->mode == ARTEA_GPU_MODE_EXACT, true, t.regs);
-    const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) * t.warps;
+    KernelFn fn = pick_kernel(r->metric, r->mode == ARTEA_GPU_MODE_EXACT, true, t.regs, t.stage != 0);
+    const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits, t.stage) * t.warps;
     if (smem > 227u * 1024u) return fail(ARTEA_GPU_EINVAL, "persistent CTA needs more than 227 KB shared memory");
     CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
@@ -285,7 +294,7 @@ struct Prepared {
 
 int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning& t, Prepared* p) {
     const bool exact = r->mode == ARTEA_GPU_MODE_EXACT;
-    KernelFn fn = pick_kernel(r->metric, exact, persistent, t.regs);
+    KernelFn fn = pick_kernel(r->metric, exact, persistent, t.regs, persistent && t.stage != 0);
     if (!fn) return fail(ARTEA_GPU_EINVAL, "unknown metric");
     a.vh_bits = t.vh_bits;
     {
@@ -304,7 +313,7 @@ int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tun
         const uint32_t needed_ctas = (a.nq + t.warps - 1) / t.warps;
         p->grid = std::min(s.ctas, needed_ctas);
         p->threads = t.warps * 32;
-        p->smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) * t.warps;
+        p->smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits, t.stage) * t.warps;
         if (int rc = ensure_slots(r, p->grid * t.warps)) return rc;
     } else {
         p->grid = a.nq;
@@ -356,7 +365,8 @@ int launch_graph(artea_gpu_router* r, SearchArgs a, bool persistent, const Tunin
     key.nq = p.a.nq;
     key.k_stride = p.a.k_stride;
     key.l0_only = p.a.l0_only;
-    key.tuning = (static_cast<uint64_t>(t.warps) << 32) | (t.vh_bits << 1) | t.regs | (persistent ? 1ull << 63 : 0);
+    key.tuning = (static_cast<uint64_t>(t.warps) << 32) | (static_cast<uint64_t>(t.stage) << 16) | (t.vh_bits << 1) |
+                 t.regs | (persistent ? 1ull << 63 : 0);
     auto it = r->graphs.find(key);
     if (it == r->graphs.end()) {
         cudaGraph_t graph = nullptr;
@@ -385,34 +395,44 @@ int launch_graph(artea_gpu_router* r, SearchArgs a, bool persistent, const Tunin
 // call's batch (one warm and one timed launch each).
 Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     Tuning t;
-    if (r->want_warps && r->want_vh_bits && r->want_regs) {
+    if (r->want_warps && r->want_vh_bits && r->want_regs && r->want_stage) {
         t.warps = r->want_warps;
         t.vh_bits = hash_bits_of(r->want_vh_bits);
         t.regs = r->want_regs == 64 ? 1u : 0u;
+        t.stage = stage_of(r->want_stage);
         return t;
     }
     const uint64_t key = (static_cast<uint64_t>(r->idx->dim) << 32) | r->cap;
     auto it = r->tuned.find(key);
     if (it != r->tuned.end()) return it->second;
-    static const uint32_t warp_choices[] = {2, 4, 8};
-    static const uint32_t bit_choices[] = {0, 8, 9, 10};
+    // Candidate lists: a fixed option is its own single choice.
+    std::vector<uint32_t> warp_choices = {2, 4, 8}, bit_choices = {0, 8, 9, 10}, reg_choices = {0, 1},
+                          stage_choices = {0, kStageRows};
+    if (r->want_warps) warp_choices = {r->want_warps};
+    if (r->want_vh_bits) bit_choices = {hash_bits_of(r->want_vh_bits)};
+    if (r->want_regs) reg_choices = {r->want_regs == 64 ? 1u : 0u};
+    if (r->want_stage) stage_choices = {stage_of(r->want_stage)};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     float best_ms = 1e30f;
     Tuning best;
-    best.warps = r->want_warps ? r->want_warps : 4;
-    best.vh_bits = r->want_vh_bits ? hash_bits_of(r->want_vh_bits) : 0;
-    for (uint32_t reg = 0; reg < 2; ++reg)
+    best.warps = warp_choices[0];
+    best.vh_bits = bit_choices[0];
+    best.regs = reg_choices[0];
+    best.stage = stage_choices[0];
+    // Row staging is timed at every register budget and warp count but only
+    // with the best table size found without it.
+    for (uint32_t stage : stage_choices)
+    for (uint32_t reg : reg_choices)
     for (uint32_t w : warp_choices) {
-        if (r->want_regs && reg != (r->want_regs == 64 ? 1u : 0u)) continue;
-        if (r->want_warps && w != r->want_warps) continue;
         for (uint32_t b : bit_choices) {
-            if (r->want_vh_bits && b != hash_bits_of(r->want_vh_bits)) continue;
+            if (stage && stage_choices.size() > 1 && bit_choices.size() > 1 && b != best.vh_bits) continue;
             Tuning c;
             c.warps = w;
             c.vh_bits = b;
             c.regs = reg;
+            c.stage = stage;
             LaunchShape s;
             if (persistent_shape(r, c, &s) != ARTEA_GPU_OK) {
                 cudaGetLastError();
@@ -451,8 +471,9 @@ int check_kernel_error(artea_gpu_router* r) {
         cudaMemsetAsync(r->d_error, 0, sizeof(int), r->stream);
         cudaStreamSynchronize(r->stream);
         static const char* what[] = {"none", "neighbour id out of range", "iteration bound exceeded",
-                                     "queue capacity exceeded", "per-query topk/queue outside the router's limits"};
-        return fail(ARTEA_GPU_EKERNEL, std::string("kernel error: ") + (h_err > 0 && h_err < 5 ? what[h_err] : "?"));
+                                     "queue capacity exceeded", "per-query topk/queue outside the router's limits",
+                                     "a bulk row copy did not complete within the wait bound"};
+        return fail(ARTEA_GPU_EKERNEL, std::string("kernel error: ") + (h_err > 0 && h_err < 6 ? what[h_err] : "?"));
     }
     return ARTEA_GPU_OK;
 }
@@ -653,6 +674,8 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
     if (o.visited_hash_bits != 0 && o.visited_hash_bits != 0xffffffffu &&
         (o.visited_hash_bits < 6 || o.visited_hash_bits > 12))
         return fail(ARTEA_GPU_EINVAL, "visited_hash_bits must be 0 (autotuned), ~0 (no table) or in [6, 12]");
+    if (o.stage_rows != 0 && o.stage_rows != 0xffffffffu && o.stage_rows != kStageRows)
+        return fail(ARTEA_GPU_EINVAL, "stage_rows must be 0 (autotuned), ~0 (vector loads) or 8");
     DeviceGuard guard(ix->device);
     auto* r = new artea_gpu_router();
     r->idx = ix;
@@ -668,6 +691,7 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
     r->want_ctas_per_sm = o.ctas_per_sm;
     r->want_vh_bits = o.visited_hash_bits;
     r->want_regs = o.register_budget;
+    r->want_stage = o.stage_rows;
     r->use_graphs = o.use_graphs != 0;
     r->words_per_slot = ((static_cast<uint64_t>(ix->n) + 127) / 128) * 4;   // multiple of 4 words
     r->list_cap = std::max<uint32_t>(std::min<uint32_t>(ix->n, 32768), 64);
@@ -803,11 +827,13 @@ int artea_gpu_router_set_early_stop(artea_gpu_router* r, const float* level_thre
 }
 
 int artea_gpu_router_tuning(const artea_gpu_router* r, uint32_t* warps_per_cta, uint32_t* visited_hash_bits,
-                            uint32_t* register_budget) {
-    if (!r || !warps_per_cta || !visited_hash_bits || !register_budget) return fail(ARTEA_GPU_EINVAL, "null argument");
+                            uint32_t* register_budget, uint32_t* stage_rows) {
+    if (!r || !warps_per_cta || !visited_hash_bits || !register_budget || !stage_rows)
+        return fail(ARTEA_GPU_EINVAL, "null argument");
     *warps_per_cta = r->last.warps;
     *visited_hash_bits = r->last.vh_bits;
     *register_budget = r->last.regs ? 64u : 85u;
+    *stage_rows = r->last.stage;
     return ARTEA_GPU_OK;
 }
 

@@ -44,7 +44,12 @@ enum : int {
     kErrBound = 2,         // an iteration bound was exceeded
     kErrQueue = 3,         // queue capacity exceeded (cannot happen for cap >= 2L)
     kErrArgs = 4,          // per-query topk/queue outside the launch's limits
+    kErrTimeout = 5,       // a bulk copy did not complete within the wait bound
 };
+
+constexpr uint32_t kStageRows = 8;          // rows per staged pass (one per row group)
+constexpr uint32_t kStagePad = 4;           // words of padding per staged row (bank spread)
+constexpr uint32_t kWaitBound = 1u << 22;   // mbarrier polls before a copy counts as lost
 
 struct DeviceGraph {
     const float* __restrict__ vecs;
@@ -200,20 +205,81 @@ __device__ __forceinline__ void accumulate(const ulonglong2 x, const ulonglong2 
     }
 }
 
+// ---------------------------------------------------------------------------
+// TMA row staging: one cp.async.bulk per candidate row into the warp's
+// shared-memory stage, completion counted on the warp's mbarrier, so a pass
+// costs one memory round trip whatever the row length.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_row_copy(uint32_t dst, const float* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+
+// Bounded wait for the phase with the given parity; false if it never came.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitBound; ++i) {
+        uint32_t ok;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+struct Stage {
+    float* buf;          // kStageRows rows of dim + kStagePad words (null: no staging)
+    uint32_t mbar;       // shared address of the warp's mbarrier
+    uint32_t phase;      // parity of the next phase to wait for
+};
+
 // Distances for cnt candidates (ids in cvid, shared memory) into cdist.
-template <int kMetric, bool kExact>
+template <int kMetric, bool kExact, bool kStage>
 __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ q, float qsq,
-                                const uint32_t* cvid, float* cdist, uint32_t cnt) {
+                                const uint32_t* cvid, float* cdist, uint32_t cnt, Stage& st, int* error) {
     const int lane = lane_id();
     const int r = lane >> 2;
     const int gi = lane & 3;
     const uint32_t dim = g.dim;
     const uint32_t nchunks = dim >> 4;
+    const uint32_t sstride = dim + kStagePad;
     for (uint32_t p = 0; p < cnt; p += 8) {
         const uint32_t idx = p + r;
         const bool valid = idx < cnt;
         const uint32_t vid = valid ? cvid[idx] : 0u;
-        const float* row = g.vecs + static_cast<size_t>(vid) * dim + 4 * gi;
+        const float* row;
+        if (kStage) {
+            // The stage's previous contents have been read by every lane
+            // (generic proxy) before the async proxy overwrites them.
+            const uint32_t nrows = min(kStageRows, cnt - p);
+            __syncwarp();
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (lane == 0) mbar_expect(st.mbar, nrows * dim * 4u);
+            __syncwarp();
+            if (static_cast<uint32_t>(lane) < nrows)
+                bulk_row_copy(smem_addr(st.buf + lane * sstride), g.vecs + static_cast<size_t>(cvid[p + lane]) * dim,
+                              dim * 4u, st.mbar);
+            if (!mbar_wait(st.mbar, st.phase)) {
+                set_error(error, kErrTimeout);
+                mbar_wait(st.mbar, st.phase);   // a second bounded wait for the copies in flight
+            }
+            st.phase ^= 1u;
+            row = st.buf + r * sstride + 4 * gi;
+        } else {
+            row = g.vecs + static_cast<size_t>(vid) * dim + 4 * gi;
+        }
         const float* qq = q + 4 * gi;
         f32x2 A01 = 0ull, A23 = 0ull;   // L2: diff^2; dot/cos: q*x   (+0.0f pairs)
         f32x2 B01 = 0ull, B23 = 0ull;   // cos: x*x
@@ -221,9 +287,8 @@ __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ 
             ulonglong2 x[kBlock];
 #pragma unroll
             for (int k = 0; k < kBlock; ++k) {
-                x[k] = (valid && cb + k < nchunks)
-                           ? __ldg(reinterpret_cast<const ulonglong2*>(row + 16 * (cb + k)))
-                           : make_ulonglong2(0ull, 0ull);
+                const ulonglong2* src = reinterpret_cast<const ulonglong2*>(row + 16 * (cb + k));
+                x[k] = (valid && cb + k < nchunks) ? (kStage ? *src : __ldg(src)) : make_ulonglong2(0ull, 0ull);
             }
 #pragma unroll
             for (int k = 0; k < kBlock; ++k) {
@@ -843,12 +908,21 @@ struct PhaseClock {
 // Shared memory words per warp for a launch.
 constexpr uint32_t kPhaseWords = 2 * kPhases;   // kPhases uint64 accumulators
 
-__host__ __device__ inline uint32_t warp_smem_words(uint32_t dim, uint32_t cap, uint32_t vh_bits) {
-    return dim + 2 * cap + 4 * kCandBatch + (vh_bits ? 4u * (1u << vh_bits) : 0u) + kPhaseWords;
+// Staged rows: a 4-word mbarrier slot, then kStageRows rows of dim + kStagePad words.
+__host__ __device__ inline uint32_t stage_words(uint32_t dim, uint32_t stage_rows) {
+    return stage_rows ? 4u + stage_rows * (dim + kStagePad) : 0u;
+}
+
+__host__ __device__ inline uint32_t warp_smem_words(uint32_t dim, uint32_t cap, uint32_t vh_bits,
+                                                    uint32_t stage_rows = 0) {
+    return dim + 2 * cap + 4 * kCandBatch + (vh_bits ? 4u * (1u << vh_bits) : 0u) + kPhaseWords +
+           stage_words(dim, stage_rows);
 }
 
 struct WarpSmem {
     unsigned long long* phase;   // kPhases accumulators (8-byte aligned: first)
+    unsigned long long* mbar;    // staging mbarrier (null without staging)
+    float* stage;                // staged rows, 16-byte aligned (null without staging)
     float* q;
     float* qd;
     uint32_t* qv;
@@ -859,10 +933,12 @@ struct WarpSmem {
     uint32_t* vh;
 };
 
-__device__ __forceinline__ WarpSmem carve(float* base, uint32_t dim, uint32_t cap) {
+__device__ __forceinline__ WarpSmem carve(float* base, uint32_t dim, uint32_t cap, uint32_t stage_rows = 0) {
     WarpSmem s;
     s.phase = reinterpret_cast<unsigned long long*>(base);
-    s.q = base + kPhaseWords;
+    s.mbar = stage_rows ? reinterpret_cast<unsigned long long*>(base + kPhaseWords) : nullptr;
+    s.stage = stage_rows ? base + kPhaseWords + 4 : nullptr;
+    s.q = base + kPhaseWords + stage_words(dim, stage_rows);
     s.qd = s.q + dim;
     s.qv = reinterpret_cast<uint32_t*>(s.qd + cap);
     s.cvid = s.qv + cap;
@@ -876,8 +952,12 @@ __device__ __forceinline__ WarpSmem carve(float* base, uint32_t dim, uint32_t ca
 // ---------------------------------------------------------------------------
 // One query (hierarchical_graph_router.hpp:195-248; query_l0_only :258-286).
 // ---------------------------------------------------------------------------
-template <int kMetric, bool kExact>
-__device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, const WarpSmem& sm) {
+// stage_phase: with kStage, the parity of the next phase of the warp's staging
+// mbarrier, which the caller initialised once (an mbarrier is not initialised
+// again while it is valid) and which carries over from query to query.
+template <int kMetric, bool kExact, bool kStage = false>
+__device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, const WarpSmem& sm,
+                           uint32_t* stage_phase = nullptr) {
     const int lane = lane_id();
     const DeviceGraph& g = a.g;
     const uint32_t dim = g.dim;
@@ -912,6 +992,10 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
     vs.spills = 0;
     uint32_t* cvid = sm.cvid;
     float* cdist = sm.cdist;
+    Stage st;
+    st.buf = sm.stage;
+    st.mbar = kStage ? smem_addr(sm.mbar) : 0u;
+    st.phase = kStage ? *stage_phase : 0u;
 
     if (g.n != 0 && g.top != kInvalidLevel && L > 0) {
         // Stage the query row in shared memory; reset the visited hash.
@@ -926,7 +1010,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
         uint32_t cur = g.entry;
         if (lane == 0) cvid[0] = cur;
         __syncwarp();
-        batch_distances<kMetric, kExact>(g, sm.q, qsq, cvid, cdist, 1);
+        batch_distances<kMetric, kExact, kStage>(g, sm.q, qsq, cvid, cdist, 1, st, a.error);
         float cur_d = cdist[0];
         ct.dist_evals = 1;
 
@@ -950,7 +1034,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                         collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error, 0u, 0u, false);
                         pos = consumed;
                         if (cnt == 0) continue;
-                        batch_distances<kMetric, kExact>(g, sm.q, qsq, cvid, cdist, cnt);
+                        batch_distances<kMetric, kExact, kStage>(g, sm.q, qsq, cvid, cdist, cnt, st, a.error);
                         ct.dist_evals += cnt;
                         ct.upper_dist_evals += cnt;
                         // First strict improvement in row order (beam_loop.hpp:153-160).
@@ -1041,7 +1125,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                 pos = consumed;
                 pc.lap(kPhCollect);
                 if (cnt == 0) continue;
-                batch_distances<kMetric, kExact>(g, sm.q, qsq, cvid, cdist, cnt);
+                batch_distances<kMetric, kExact, kStage>(g, sm.q, qsq, cvid, cdist, cnt, st, a.error);
                 ct.dist_evals += cnt;
                 pc.lap(kPhDist);
                 if (p2 >= 0 && !pf_have_ids) {
@@ -1092,6 +1176,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
         s.visited_spills = vs.spills;
         a.stats[qi] = s;
     }
+    if (kStage) *stage_phase = st.phase;
     __syncwarp();
 }
 
@@ -1109,19 +1194,30 @@ __global__ void __launch_bounds__(32, 24) search_plain_kernel(SearchArgs a) {
 // Persistent schedule: warps pull query indices from a shared counter.
 // kMinBlocks sets the register budget: 4 blocks of 256 threads per SM caps a
 // thread at 64 registers (32 resident warps), 3 at 85 (24 warps).
-template <int kMetric, bool kExact, int kMinBlocks>
+template <int kMetric, bool kExact, int kMinBlocks, bool kStage = false>
 __global__ void __launch_bounds__(256, kMinBlocks) search_persistent_kernel(SearchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
-    const WarpSmem sm = carve(smem + static_cast<size_t>(warp) * warp_smem_words(a.g.dim, a.cap, a.vh_bits),
-                              a.g.dim, a.cap);
+    const uint32_t stage_rows = kStage ? kStageRows : 0u;
+    const WarpSmem sm = carve(smem + static_cast<size_t>(warp) * warp_smem_words(a.g.dim, a.cap, a.vh_bits,
+                                                                                    stage_rows),
+                              a.g.dim, a.cap, stage_rows);
+    uint32_t stage_phase = 0u;
+    if (kStage) {
+        if (lane_id() == 0) mbar_init(smem_addr(sm.mbar));
+        __syncwarp();
+    }
     for (;;) {
         uint32_t qi = 0;
         if (lane_id() == 0) qi = atomicAdd(a.next_query, 1u);
         qi = __shfl_sync(kFull, qi, 0);
         if (qi >= a.nq) break;
-        search_one<kMetric, kExact>(a, qi, slot, sm);
+        search_one<kMetric, kExact, kStage>(a, qi, slot, sm, &stage_phase);
+    }
+    if (kStage) {
+        __syncwarp();
+        if (lane_id() == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(sm.mbar)) : "memory");
     }
 }
 

@@ -183,7 +183,7 @@ class GpuRouter:
     def __init__(self, index: DeviceIndex, metric, topk: int, candidate_queue_size: int, mode: str = "exact",
                  schedule: str = "auto", warps_per_cta: int = 0, ctas_per_sm: int = 0, max_batch: int = 0,
                  max_queue: int = 0, visited_hash_bits: int = 0, register_budget: int = 0,
-                 use_graphs: bool = False):
+                 use_graphs: bool = False, stage_rows: int = 0):
         opts = nat.RouterOpts()
         opts.metric = metric_code(metric)
         opts.mode = MODES[mode] if isinstance(mode, str) else int(mode)
@@ -194,6 +194,7 @@ class GpuRouter:
         opts.max_queue = max_queue
         opts.visited_hash_bits = visited_hash_bits
         opts.register_budget = register_budget
+        opts.stage_rows = stage_rows
         opts.use_graphs = 1 if use_graphs else 0
         h = ctypes.c_void_p()
         nat.check(nat.lib().artea_gpu_router_create(index.handle, topk, candidate_queue_size, ctypes.byref(opts),
@@ -266,9 +267,11 @@ class GpuRouter:
 
     def tuning(self) -> dict:
         """Launch parameters of the last launch (the autotuner's pick)."""
-        w, b, g = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
-        nat.check(nat.lib().artea_gpu_router_tuning(self._h, ctypes.byref(w), ctypes.byref(b), ctypes.byref(g)))
-        return {"warps_per_cta": w.value, "visited_hash_bits": b.value, "register_budget": g.value}
+        w, b, g, st = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        nat.check(nat.lib().artea_gpu_router_tuning(self._h, ctypes.byref(w), ctypes.byref(b), ctypes.byref(g),
+                                                    ctypes.byref(st)))
+        return {"warps_per_cta": w.value, "visited_hash_bits": b.value, "register_budget": g.value,
+                "stage_rows": st.value}
 
     def launches(self) -> int:
         n = ctypes.c_uint64()

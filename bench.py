@@ -431,6 +431,7 @@ def main() -> None:
     ap.add_argument("--profile-warps", type=int, default=4)
     ap.add_argument("--profile-vh-bits", type=int, default=-1, help="-1: no shared-memory visited hash")
     ap.add_argument("--profile-regs", type=int, default=85)
+    ap.add_argument("--profile-stage", type=int, default=-1, help="-1: vector loads; 8: TMA-staged rows")
     ap.add_argument("--phases", action="store_true", help="with --profile: per-phase cycle breakdown")
     ap.add_argument("--uneven", action="store_true",
                     help="per-query topk in {10,100} and queue in {64,128,256,512} in one launch (the default for "
@@ -476,7 +477,8 @@ def main() -> None:
                       schedule="plain" if args.schedule == "plain" else "persistent",
                       warps_per_cta=args.profile_warps,
                       visited_hash_bits=args.profile_vh_bits if args.profile_vh_bits >= 0 else 0xFFFFFFFF,
-                      register_budget=args.profile_regs, max_batch=nq)
+                      register_budget=args.profile_regs, max_batch=nq,
+                      stage_rows=args.profile_stage if args.profile_stage >= 0 else 0xFFFFFFFF)
         s = torch.cuda.current_stream(device)
         phases = torch.zeros((nq, 8), dtype=torch.int64, device=device) if args.phases else None
         for rep in range(2):

@@ -147,6 +147,10 @@ typedef struct artea_gpu_router_opts {
                                    0xFFFFFFFF = no table (HBM bitset only) */
     uint32_t register_budget;   /* registers per thread of the persistent kernel:
                                    64 or 85; 0 = autotuned */
+    uint32_t stage_rows;        /* persistent kernel's row reads: 8 = each pass's
+                                   candidate rows staged in shared memory by TMA
+                                   bulk copies; 0xFFFFFFFF = vector loads from
+                                   HBM/L2; 0 = autotuned */
 } artea_gpu_router_opts;
 
 /* Library / device information. */
@@ -263,9 +267,10 @@ int artea_gpu_centroid_entry(const artea_gpu_index* index, int metric, const uin
  * turns it off. No reference counterpart (measurement only). */
 int artea_gpu_router_set_phase_buffer(artea_gpu_router* router, void* d_phase_cycles);
 
-/* Launch parameters of the router's last launch (the autotuner's choice). */
+/* Launch parameters of the router's last launch (the autotuner's choice);
+ * stage_rows 0 = vector loads, 8 = TMA-staged rows. */
 int artea_gpu_router_tuning(const artea_gpu_router* router, uint32_t* warps_per_cta, uint32_t* visited_hash_bits,
-                            uint32_t* register_budget);
+                            uint32_t* register_budget, uint32_t* stage_rows);
 
 /* ---- Serving loop (continuous batching) ----
  * No counterpart in the reference, whose batch_query is one blocking call; each

@@ -207,7 +207,43 @@ def test_exact_with_visited_hash_spill_and_register_budgets(sift20k, vh_bits, re
         np.testing.assert_array_equal(out, ref, err_msg=f"vh_bits={vh_bits} regs={regs} warps={warps}")
         if vh_bits == 6:
             assert (st[:, 7] > 0).all(), "expected every query to spill to the bitset"
-        assert r.tuning() == {"warps_per_cta": warps, "visited_hash_bits": vh_bits, "register_budget": regs}
+        assert r.tuning() == {"warps_per_cta": warps, "visited_hash_bits": vh_bits, "register_budget": regs,
+                              "stage_rows": 0}
+
+
+@pytest.mark.parametrize("regs", [64, 85])
+def test_tma_staged_rows_are_bit_exact(sift20k, regs):
+    # Rows staged in shared memory by cp.async.bulk (one copy per row, one
+    # mbarrier per warp) must leave ids, distances and counters unchanged.
+    g, base, queries = sift20k
+    idx = DeviceIndex(g, base)
+    nq = queries.shape[0]
+    rng = np.random.default_rng(5)
+    topk = rng.choice(np.array([10, 100], np.uint32), nq)
+    queue = np.maximum(rng.choice(np.array([64, 128, 256], np.uint32), nq), topk)
+    ref, ost = orc.batch_query(g, base, queries, topk, queue, metric=0, k_stride=100, stats=True)
+    # ctas_per_sm=1 leaves fewer warps than queries: every warp runs several
+    # queries on the same staging mbarrier.
+    for warps, vh, ctas in ((2, 8, 0), (4, 0xFFFFFFFF, 0), (2, 8, 1)):
+        r = GpuRouter(idx, 0, 100, 256, mode="exact", schedule="persistent", warps_per_cta=warps,
+                      visited_hash_bits=vh, register_budget=regs, stage_rows=8, ctas_per_sm=ctas)
+        out, st = r.batch_query(queries, topk=topk, queue=queue, k_stride=100, stats=True)
+        np.testing.assert_array_equal(out, ref, err_msg=f"staged warps={warps} vh={vh}")
+        np.testing.assert_array_equal(st[:, :7], ost[:, :7])
+        assert r.tuning()["stage_rows"] == 8
+        r.close()
+
+
+@pytest.mark.parametrize("name", ["deep1k_cos", "gist400", "axis80"])
+def test_tma_staged_rows_match_reference(name):
+    c = golden_case(name)
+    idx = index_for(name)
+    for L in c.queues:
+        r = GpuRouter(idx, c.metric, c.topk, L, mode="exact", schedule="persistent", stage_rows=8)
+        out, st = r.batch_query(c.queries, stats=True)
+        np.testing.assert_array_equal(out, c.words[L], err_msg=f"{name} L={L} staged")
+        np.testing.assert_array_equal(st[:, 0].astype(np.uint64), c.calls[L])
+        r.close()
 
 
 def test_plain_schedule_spill(sift20k):
