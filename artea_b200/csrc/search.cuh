@@ -754,28 +754,39 @@ __device__ inline void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, 
         const bool improving = valid && d < lim;
         uint32_t imask = __ballot_sync(kFull, improving);
         if (imask == 0 && improving_before == 0) continue;
-        // pre = #{i < j : d_i <= d_j}: earlier chunks from shared memory, this
-        // chunk by shuffles over the improving lanes only.
-        uint32_t pre = 0;
-        if (improving_before) {
-            for (uint32_t i = 0; i < base; ++i) pre += cdist[i] <= d ? 1u : 0u;
-        }
-        for (uint32_t bits = imask & lt_mask; __any_sync(kFull, bits != 0);) {
-            // each lane walks its own set of earlier improving lanes; shuffles
-            // need every lane, so lanes take turns through a uniform loop.
-            const int k = bits ? __ffs(bits) - 1 : 0;
-            const float dk = __shfl_sync(kFull, d, k);
-            if (bits) {
-                pre += dk <= d ? 1u : 0u;
-                bits &= bits - 1;
-            }
-        }
         // #{e in T : e.dist <= d} < L - pre  <=>  T[L-pre-1].dist > d (or T is
-        // shorter than L-pre).
+        // shorter than L-pre). pre = #{i < j : d_i <= d_j} is at most ub, the
+        // number of earlier improving candidates, and the test is monotone in
+        // pre: a lane accepted with ub is accepted, and only lanes it leaves
+        // undecided need the exact count.
+        const uint32_t ub = improving_before + __popc(imask & lt_mask);
         bool acc = false;
-        if (improving && pre < q.L) {
-            const uint32_t idx = q.L - pre - 1;
+        if (improving && ub < q.L) {
+            const uint32_t idx = q.L - ub - 1;
             acc = idx >= tn || q.d[idx] > d;
+        }
+        const bool undecided = improving && !acc && ub != 0;
+        if (__any_sync(kFull, undecided)) {
+            // Exact pre: earlier chunks from shared memory, this chunk by
+            // shuffles over the improving lanes only.
+            uint32_t pre = 0;
+            if (improving_before) {
+                for (uint32_t i = 0; i < base; ++i) pre += cdist[i] <= d ? 1u : 0u;
+            }
+            for (uint32_t bits = imask & lt_mask; __any_sync(kFull, bits != 0);) {
+                // each lane walks its own set of earlier improving lanes; shuffles
+                // need every lane, so lanes take turns through a uniform loop.
+                const int k = bits ? __ffs(bits) - 1 : 0;
+                const float dk = __shfl_sync(kFull, d, k);
+                if (bits) {
+                    pre += dk <= d ? 1u : 0u;
+                    bits &= bits - 1;
+                }
+            }
+            if (undecided && pre < q.L) {
+                const uint32_t idx = q.L - pre - 1;
+                acc = idx >= tn || q.d[idx] > d;
+            }
         }
         const uint32_t b = __ballot_sync(kFull, acc);
         if (acc) {
