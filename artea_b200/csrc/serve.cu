@@ -30,13 +30,19 @@ using namespace artea_gpu;
 namespace {
 
 struct ServeCtl {
-    uint32_t* head;                   // next sequence to claim (device)
+    unsigned long long* head;         // (closed << 32) | next sequence to claim (device; claimed by CAS)
     const volatile uint32_t* tail;    // sequences published so far (device, written by host copies)
     const volatile uint32_t* stop;    // set by the host to end the kernel
     volatile uint32_t* done;          // mapped host memory: done[slot] = seq + 1 when finished
     uint32_t ring;                    // ring slots; slot = seq % ring
-    uint32_t idle_limit;              // idle polls (about 1 us each) before the kernel exits
+    uint32_t idle_limit;              // microseconds without work before the kernel exits
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
 
 template <int kMetric, bool kExact>
 __global__ void __launch_bounds__(256, 3) serve_kernel(SearchArgs a, ServeCtl c) {
@@ -46,30 +52,59 @@ __global__ void __launch_bounds__(256, 3) serve_kernel(SearchArgs a, ServeCtl c)
     const uint32_t wslot = blockIdx.x * (blockDim.x >> 5) + warp;
     const WarpSmem sm = carve(smem + static_cast<size_t>(warp) * warp_smem_words(a.g.dim, a.cap, a.vh_bits),
                               a.g.dim, a.cap);
-    uint32_t idle = 0;
+    // Idle warps only read head and tail (no atomics) and back off, so the
+    // few warps with work are not slowed by thousands polling one address.
+    // A kernel instance ends as a whole: the first warp idle for idle_limit
+    // microseconds closes the ring for it (the high word of head) while it is
+    // empty; every warp then exits once its current query is done, and the
+    // host relaunches (reopening the ring) when new work is pending. Warps
+    // never leave one by one, which would leave a running kernel with too few
+    // warps for the next burst.
+    const volatile unsigned long long* vhead = c.head;
+    unsigned long long idle_since = 0;
+    uint32_t backoff = 64;
     for (;;) {
         uint32_t seq = 0;
-        int got = 0;
+        int state = 0;   // 0: nothing claimed, 1: claimed seq, 2: ring closed
         if (lane == 0) {
             for (int tries = 0; tries < 64; ++tries) {
-                const uint32_t h = atomicAdd(c.head, 0u);
+                const unsigned long long cur = *vhead;
+                if (cur >> 32) {
+                    state = 2;
+                    break;
+                }
+                const uint32_t h = static_cast<uint32_t>(cur);
                 const uint32_t t = *c.tail;
                 if (static_cast<int32_t>(t - h) <= 0) break;
-                if (atomicCAS(c.head, h, h + 1u) == h) {
+                if (atomicCAS(c.head, cur, cur + 1ull) == cur) {
                     seq = h;
-                    got = 1;
+                    state = 1;
                     break;
                 }
             }
         }
-        got = __shfl_sync(kFull, got, 0);
+        state = __shfl_sync(kFull, state, 0);
         seq = __shfl_sync(kFull, seq, 0);
-        if (!got) {
-            if (*c.stop || ++idle > c.idle_limit) break;
-            __nanosleep(1000);
+        if (state == 2 || *c.stop) break;
+        if (state == 0) {
+            const unsigned long long now = global_ns();
+            if (idle_since == 0) idle_since = now;
+            if (now - idle_since > 1000ull * c.idle_limit) {
+                if (lane == 0) {
+                    const unsigned long long cur = *vhead;
+                    const uint32_t t = *c.tail;
+                    if (!(cur >> 32) && static_cast<int32_t>(t - static_cast<uint32_t>(cur)) <= 0)
+                        atomicCAS(c.head, cur, cur | (1ull << 32));
+                }
+                __syncwarp();
+                continue;   // the next look sees the closed ring, or new work
+            }
+            __nanosleep(backoff);
+            backoff = min(backoff * 2u, 16384u);
             continue;
         }
-        idle = 0;
+        idle_since = 0;
+        backoff = 64;
         // The ring row was written before `tail` advanced (one copy stream);
         // order this warp's reads after the observation of `tail`.
         __threadfence();
@@ -116,7 +151,7 @@ struct artea_gpu_server {
     float* d_q = nullptr;
     uint32_t* d_topk = nullptr;
     uint32_t* d_queue = nullptr;
-    uint32_t* d_ctl = nullptr;       // [head, tail, stop, pad]
+    uint32_t* d_ctl = nullptr;       // [head, closed, tail, stop]: head/closed one 64-bit word
     uint32_t* d_vis_bits = nullptr;
     uint32_t* d_vis_list = nullptr;
     int* d_error = nullptr;
@@ -169,14 +204,17 @@ int launch_serving(artea_gpu_server* s) {
     a.error = s->d_error;
     a.coherent = 1;
     ServeCtl c;
-    c.head = s->d_ctl;
-    c.tail = s->d_ctl + 1;
-    c.stop = s->d_ctl + 2;
+    c.head = reinterpret_cast<unsigned long long*>(s->d_ctl);
+    c.tail = s->d_ctl + 2;
+    c.stop = s->d_ctl + 3;
     c.done = s->d_done_alias;
     c.ring = s->ring;
     c.idle_limit = s->idle_limit;
     CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(s->fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(s->smem)));
+    // Reopen the ring (the previous instance closed it before exiting); same
+    // stream, so after that instance and before this one.
+    CUDA_TRY(cudaMemsetAsync(s->d_ctl + 1, 0, sizeof(uint32_t), s->kstream));
     s->fn<<<s->grid, s->warps * 32, s->smem, s->kstream>>>(a, c);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaEventRecord(s->kdone, s->kstream));
@@ -238,7 +276,7 @@ extern "C" int artea_gpu_server_create(artea_gpu_index* ix, const artea_gpu_serv
     s->ring = o.ring_slots;
     s->warps = o.warps_per_cta ? o.warps_per_cta : 2;
     if (s->warps > 8) return cleanup(fail(ARTEA_GPU_EINVAL, "warps_per_cta must be <= 8"));
-    s->idle_limit = o.idle_polls ? o.idle_polls : 5000;
+    s->idle_limit = o.idle_polls ? o.idle_polls : 5000;   // microseconds
     s->cap = std::max<uint32_t>(2u * s->qmax, 2u);
     uint32_t kb = 1;
     while (kb < 32 && (1ull << kb) < ix->n) ++kb;
@@ -333,7 +371,7 @@ extern "C" int artea_gpu_server_submit(artea_gpu_server* s, const float* queries
     // Publish: the new tail value is copied from pageable memory (captured at
     // the call), ordered after the row copies on the same stream.
     uint32_t new_tail = static_cast<uint32_t>(seq0 + n);
-    CUDA_TRY(cudaMemcpyAsync(s->d_ctl + 1, &new_tail, sizeof(uint32_t), cudaMemcpyHostToDevice, s->cstream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_ctl + 2, &new_tail, sizeof(uint32_t), cudaMemcpyHostToDevice, s->cstream));
     s->next_seq = seq0 + n;
     *ticket = seq0;
     return ensure_running(s);
@@ -379,7 +417,7 @@ extern "C" int artea_gpu_server_destroy(artea_gpu_server* s) {
     DeviceGuard guard(s->idx->device);
     if (s->d_ctl) {
         const uint32_t one = 1;
-        cudaMemcpy(s->d_ctl + 2, &one, sizeof(uint32_t), cudaMemcpyHostToDevice);
+        cudaMemcpy(s->d_ctl + 3, &one, sizeof(uint32_t), cudaMemcpyHostToDevice);
     }
     if (s->kstream) cudaStreamSynchronize(s->kstream);
     if (s->cstream) cudaStreamSynchronize(s->cstream);
