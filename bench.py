@@ -168,17 +168,22 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def profile_traffic(workload: str):
-    """dram read+write bytes per launch from the committed ncu summary, if any."""
+def profile_traffic(workload: str, queue=None):
+    """dram read+write bytes per launch from the committed ncu summary of this
+    workload: the line for this queue size (traffic_bytes_per_launch_L<queue>:)
+    if there is one, else the workload's default line (traffic_bytes_per_launch:)."""
     p = os.path.join(ROOT, "profiles", f"search_kernel_{workload}.md")
     if not os.path.exists(p):
         return None
-    for line in open(p):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
+    keys = ([f"traffic_bytes_per_launch_L{queue}:"] if queue is not None else []) + ["traffic_bytes_per_launch:"]
+    lines = [line.strip() for line in open(p)]
+    for key in keys:
+        for line in lines:
+            if line.startswith(key):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
     return None
 
 
@@ -614,7 +619,7 @@ def main() -> None:
 
     peaks = measured_peaks()
     achieved = alg_bytes / (mean_ms / 1e3) / 1e9
-    traffic = profile_traffic(w.name)
+    traffic = profile_traffic(w.name, chosen)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peaks["source"],
