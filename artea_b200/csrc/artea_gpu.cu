@@ -43,7 +43,7 @@ struct LaunchShape {
 struct Tuning {
     uint32_t warps = 4;
     uint32_t vh_bits = 11;
-    uint32_t regs = 0;   // 0: 85-register budget, 1: 64-register budget
+    uint32_t regs = 0;   // 0: 85-register budget, 1: 64, 2: 96 (CTAs of at most 4 warps)
     uint32_t stage = 0;  // 0: rows read with vector loads; kStageRows: TMA-staged in shared memory
 };
 
@@ -141,15 +141,26 @@ uint32_t stage_of(uint32_t want) { return want == kNoHash ? 0u : kStageRows; }
 
 using KernelFn = void (*)(SearchArgs);
 
-// regs: 0 = 85-register budget, 1 = 64-register budget (persistent only);
-// stage: rows staged in shared memory by TMA (persistent only).
+// regs: 0 = 85-register budget (80 registers, 24 warps per SM), 1 = 64,
+// 2 = 96 (CTAs of at most 4 warps) (persistent only); stage: rows staged in
+// shared memory by TMA.
+template <int kMetric, bool kExact, bool kStage>
+KernelFn pick_persistent_s(uint32_t regs) {
+    switch (regs) {
+        case 1: return search_persistent_kernel<kMetric, kExact, 64, kStage>;
+        case 2: return search_persistent_kernel<kMetric, kExact, 96, kStage>;
+        default: return search_persistent_kernel<kMetric, kExact, 85, kStage>;
+    }
+}
+
 template <int kMetric, bool kExact>
 KernelFn pick_persistent(uint32_t regs, bool stage) {
-    if (stage)
-        return regs == 1 ? search_persistent_kernel<kMetric, kExact, 4, true>
-                         : search_persistent_kernel<kMetric, kExact, 3, true>;
-    return regs == 1 ? search_persistent_kernel<kMetric, kExact, 4> : search_persistent_kernel<kMetric, kExact, 3>;
+    return stage ? pick_persistent_s<kMetric, kExact, true>(regs) : pick_persistent_s<kMetric, kExact, false>(regs);
 }
+
+// Router option register_budget (64, 85, 96) <-> Tuning::regs (1, 0, 2).
+uint32_t regs_index(uint32_t budget) { return budget == 64 ? 1u : (budget == 96 ? 2u : 0u); }
+uint32_t regs_budget(uint32_t index) { return index == 1 ? 64u : (index == 2 ? 96u : 85u); }
 
 template <int kMetric>
 KernelFn pick_kernel_m(bool exact, bool persistent, uint32_t regs, bool stage) {
@@ -225,6 +236,8 @@ int persistent_shape(artea_gpu_router* r, const Tuning& t, LaunchShape* s) {
         *s = hit->second;
         return ARTEA_GPU_OK;
     }
+    if (t.regs == 2 && t.warps > 4)
+        return fail(ARTEA_GPU_EINVAL, "register budget 96 allows at most 4 warps per CTA");
     KernelFn fn = pick_kernel(r->metric, r->mode == ARTEA_GPU_MODE_EXACT, true, t.regs, t.stage != 0);
     const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits, t.stage) * t.warps;
     if (smem > 227u * 1024u) return fail(ARTEA_GPU_EINVAL, "persistent CTA needs more than 227 KB shared memory");
@@ -398,7 +411,7 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     if (r->want_warps && r->want_vh_bits && r->want_regs && r->want_stage) {
         t.warps = r->want_warps;
         t.vh_bits = hash_bits_of(r->want_vh_bits);
-        t.regs = r->want_regs == 64 ? 1u : 0u;
+        t.regs = regs_index(r->want_regs);
         t.stage = stage_of(r->want_stage);
         return t;
     }
@@ -406,11 +419,11 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     auto it = r->tuned.find(key);
     if (it != r->tuned.end()) return it->second;
     // Candidate lists: a fixed option is its own single choice.
-    std::vector<uint32_t> warp_choices = {2, 4, 8}, bit_choices = {0, 8, 9, 10}, reg_choices = {0, 1},
+    std::vector<uint32_t> warp_choices = {2, 4, 8}, bit_choices = {0, 8, 9, 10}, reg_choices = {0, 1, 2},
                           stage_choices = {0, kStageRows};
     if (r->want_warps) warp_choices = {r->want_warps};
     if (r->want_vh_bits) bit_choices = {hash_bits_of(r->want_vh_bits)};
-    if (r->want_regs) reg_choices = {r->want_regs == 64 ? 1u : 0u};
+    if (r->want_regs) reg_choices = {regs_index(r->want_regs)};
     if (r->want_stage) stage_choices = {stage_of(r->want_stage)};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -669,8 +682,8 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
     if (o.mode != ARTEA_GPU_MODE_EXACT && o.mode != ARTEA_GPU_MODE_FAST) return fail(ARTEA_GPU_EINVAL, "unknown mode");
     if (o.schedule < 0 || o.schedule > 2) return fail(ARTEA_GPU_EINVAL, "unknown schedule");
     if (o.warps_per_cta > 8) return fail(ARTEA_GPU_EINVAL, "warps_per_cta must be <= 8");
-    if (o.register_budget != 0 && o.register_budget != 64 && o.register_budget != 85)
-        return fail(ARTEA_GPU_EINVAL, "register_budget must be 0 (autotuned), 64 or 85");
+    if (o.register_budget != 0 && o.register_budget != 64 && o.register_budget != 85 && o.register_budget != 96)
+        return fail(ARTEA_GPU_EINVAL, "register_budget must be 0 (autotuned), 64, 85 or 96");
     if (o.visited_hash_bits != 0 && o.visited_hash_bits != 0xffffffffu &&
         (o.visited_hash_bits < 6 || o.visited_hash_bits > 12))
         return fail(ARTEA_GPU_EINVAL, "visited_hash_bits must be 0 (autotuned), ~0 (no table) or in [6, 12]");
@@ -832,7 +845,7 @@ int artea_gpu_router_tuning(const artea_gpu_router* r, uint32_t* warps_per_cta, 
         return fail(ARTEA_GPU_EINVAL, "null argument");
     *warps_per_cta = r->last.warps;
     *visited_hash_bits = r->last.vh_bits;
-    *register_budget = r->last.regs ? 64u : 85u;
+    *register_budget = regs_budget(r->last.regs);
     *stage_rows = r->last.stage;
     return ARTEA_GPU_OK;
 }

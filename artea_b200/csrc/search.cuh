@@ -1203,10 +1203,16 @@ __global__ void __launch_bounds__(32, 24) search_plain_kernel(SearchArgs a) {
 }
 
 // Persistent schedule: warps pull query indices from a shared counter.
-// kMinBlocks sets the register budget: 4 blocks of 256 threads per SM caps a
-// thread at 64 registers (32 resident warps), 3 at 85 (24 warps).
-template <int kMetric, bool kExact, int kMinBlocks, bool kStage = false>
-__global__ void __launch_bounds__(256, kMinBlocks) search_persistent_kernel(SearchArgs a) {
+// kBudget sets the register budget through the launch bounds: 64 (4 CTAs of
+// 256 threads per SM, 32 resident warps), 85 (3 x 256: 80 registers used, 24
+// warps) or 96 (5 CTAs of at most 128 threads: 20 warps, the search state
+// without spills). (__maxnreg__ with the same counts measured slower.)
+constexpr int budget_threads(int budget) { return budget == 96 ? 128 : 256; }
+constexpr int budget_min_blocks(int budget) { return budget == 64 ? 4 : (budget == 96 ? 5 : 3); }
+
+template <int kMetric, bool kExact, int kBudget, bool kStage = false>
+__global__ void __launch_bounds__(budget_threads(kBudget), budget_min_blocks(kBudget))
+    search_persistent_kernel(SearchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;

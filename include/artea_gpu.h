@@ -146,7 +146,9 @@ typedef struct artea_gpu_router_opts {
                                    bucket), in [6, 12]; 0 = autotuned;
                                    0xFFFFFFFF = no table (HBM bitset only) */
     uint32_t register_budget;   /* registers per thread of the persistent kernel:
-                                   64 or 85; 0 = autotuned */
+                                   64 (32 warps per SM), 85 (80 used, 24
+                                   warps) or 96 (20 warps; CTAs of at most 4
+                                   warps); 0 = autotuned */
     uint32_t stage_rows;        /* persistent kernel's row reads: 8 = each pass's
                                    candidate rows staged in shared memory by TMA
                                    bulk copies; 0xFFFFFFFF = vector loads from

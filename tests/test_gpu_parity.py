@@ -193,15 +193,15 @@ def test_topk_larger_than_found_keeps_invalid_tail():
     assert (entry_vids(out[:, 4:]) == 0x7FFFFFFF).all()
 
 
-@pytest.mark.parametrize("vh_bits,regs", [(6, 64), (6, 85), (10, 64), (10, 85)])
+@pytest.mark.parametrize("vh_bits,regs", [(6, 64), (6, 85), (10, 85), (10, 96)])
 def test_exact_with_visited_hash_spill_and_register_budgets(sift20k, vh_bits, regs):
     # vh_bits=6 is a 64-bucket (512-slot) table, so every query here sends
     # ids of full buckets to the HBM bitset; results must not change.
     g, base, queries = sift20k
     idx = DeviceIndex(g, base)
-    for warps in (2, 8):
+    for warps in ((2, 4) if regs == 96 else (2, 8)):   # budget 96: CTAs of at most 4 warps
         r = GpuRouter(idx, 0, 100, 200, mode="exact", schedule="persistent", warps_per_cta=warps,
-                      visited_hash_bits=vh_bits, register_budget=regs)
+                      visited_hash_bits=vh_bits, register_budget=regs, stage_rows=0xFFFFFFFF)
         out, st = r.batch_query(queries[:200], stats=True)
         ref = orc.batch_query(g, base, queries[:200], 100, 200, metric=0)
         np.testing.assert_array_equal(out, ref, err_msg=f"vh_bits={vh_bits} regs={regs} warps={warps}")
@@ -211,7 +211,7 @@ def test_exact_with_visited_hash_spill_and_register_budgets(sift20k, vh_bits, re
                               "stage_rows": 0}
 
 
-@pytest.mark.parametrize("regs", [64, 85])
+@pytest.mark.parametrize("regs", [64, 85, 96])
 def test_tma_staged_rows_are_bit_exact(sift20k, regs):
     # Rows staged in shared memory by cp.async.bulk (one copy per row, one
     # mbarrier per warp) must leave ids, distances and counters unchanged.
