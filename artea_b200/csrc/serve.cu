@@ -34,6 +34,7 @@ struct ServeCtl {
     const volatile uint32_t* tail;    // sequences published so far (device, written by host copies)
     const volatile uint32_t* stop;    // set by the host to end the kernel
     volatile uint32_t* done;          // mapped host memory: done[slot] = seq + 1 when finished
+    volatile uint32_t* closed;        // mapped host memory: set to 1 by the warp that closes the ring
     uint32_t ring;                    // ring slots; slot = seq % ring
     uint32_t idle_limit;              // microseconds without work before the kernel exits
 };
@@ -93,8 +94,14 @@ __global__ void __launch_bounds__(256, 3) serve_kernel(SearchArgs a, ServeCtl c)
                 if (lane == 0) {
                     const unsigned long long cur = *vhead;
                     const uint32_t t = *c.tail;
-                    if (!(cur >> 32) && static_cast<int32_t>(t - static_cast<uint32_t>(cur)) <= 0)
-                        atomicCAS(c.head, cur, cur | (1ull << 32));
+                    if (!(cur >> 32) && static_cast<int32_t>(t - static_cast<uint32_t>(cur)) <= 0 &&
+                        atomicCAS(c.head, cur, cur | (1ull << 32)) == cur) {
+                        // Tell the host this instance is ending (it relaunches
+                        // on the same stream, after this instance, when work
+                        // is pending).
+                        *c.closed = 1u;
+                        __threadfence_system();
+                    }
                 }
                 __syncwarp();
                 continue;   // the next look sees the closed ring, or new work
@@ -147,6 +154,8 @@ struct artea_gpu_server {
     cudaStream_t kstream = nullptr, cstream = nullptr;
     cudaEvent_t kdone = nullptr;
     bool launched = false;
+    uint32_t* h_closed = nullptr;       // mapped: the running instance closed its ring
+    uint32_t* d_closed_alias = nullptr;
     // device ring and control
     float* d_q = nullptr;
     uint32_t* d_topk = nullptr;
@@ -208,6 +217,7 @@ int launch_serving(artea_gpu_server* s) {
     c.tail = s->d_ctl + 2;
     c.stop = s->d_ctl + 3;
     c.done = s->d_done_alias;
+    c.closed = s->d_closed_alias;
     c.ring = s->ring;
     c.idle_limit = s->idle_limit;
     CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(s->fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -232,13 +242,17 @@ bool all_done(const artea_gpu_server* s, uint64_t seq0, uint32_t n) {
     return true;
 }
 
-// Relaunch the kernel if published work is pending and it has exited.
+// Relaunch the kernel if published work is pending and the running instance
+// has closed its ring. The instance's own closing flag (mapped host memory)
+// decides, not an event on its stream: the new instance is queued on the same
+// stream and starts once the old one has drained.
 int ensure_running(artea_gpu_server* s) {
     if (s->next_seq == s->consumed_upto) return ARTEA_GPU_OK;
     if (s->launched) {
+        if (*static_cast<volatile uint32_t*>(s->h_closed) == 0u) return ARTEA_GPU_OK;
         const cudaError_t q = cudaEventQuery(s->kdone);
-        if (q == cudaErrorNotReady) return ARTEA_GPU_OK;
-        if (q != cudaSuccess) return fail(ARTEA_GPU_ECUDA, std::string("serving kernel: ") + cudaGetErrorString(q));
+        if (q != cudaSuccess && q != cudaErrorNotReady)
+            return fail(ARTEA_GPU_ECUDA, std::string("serving kernel: ") + cudaGetErrorString(q));
         int h_err = 0;
         CUDA_TRY(cudaMemcpy(&h_err, s->d_error, sizeof(int), cudaMemcpyDeviceToHost));
         if (h_err) return fail(ARTEA_GPU_EKERNEL, "serving kernel error " + std::to_string(h_err));
@@ -249,6 +263,7 @@ int ensure_running(artea_gpu_server* s) {
         if (!s->consumed[seq % s->ring] && s->h_done[seq % s->ring] != static_cast<uint32_t>(seq + 1)) pending = true;
     }
     if (!pending) return ARTEA_GPU_OK;
+    *static_cast<volatile uint32_t*>(s->h_closed) = 0u;
     return launch_serving(s);
 }
 
@@ -276,7 +291,11 @@ extern "C" int artea_gpu_server_create(artea_gpu_index* ix, const artea_gpu_serv
     s->ring = o.ring_slots;
     s->warps = o.warps_per_cta ? o.warps_per_cta : 2;
     if (s->warps > 8) return cleanup(fail(ARTEA_GPU_EINVAL, "warps_per_cta must be <= 8"));
-    s->idle_limit = o.idle_polls ? o.idle_polls : 5000;   // microseconds
+    // One second by default: a kernel instance that ends and a new one queued
+    // behind it on the same stream has, under relaunches every few
+    // milliseconds, been seen to leave the new one waiting (the old one's warps
+    // had all exited); a long idle window keeps relaunches to quiet periods.
+    s->idle_limit = o.idle_polls ? o.idle_polls : 1000000;   // microseconds
     s->cap = std::max<uint32_t>(2u * s->qmax, 2u);
     uint32_t kb = 1;
     while (kb < 32 && (1ull << kb) < ix->n) ++kb;
@@ -317,11 +336,14 @@ extern "C" int artea_gpu_server_create(artea_gpu_index* ix, const artea_gpu_serv
         cudaHostAlloc(reinterpret_cast<void**>(&s->h_out), sizeof(uint64_t) * s->ring * s->kmax, cudaHostAllocMapped) !=
             cudaSuccess ||
         cudaHostAlloc(reinterpret_cast<void**>(&s->h_done), sizeof(uint32_t) * s->ring, cudaHostAllocMapped) !=
-            cudaSuccess)
+            cudaSuccess ||
+        cudaHostAlloc(reinterpret_cast<void**>(&s->h_closed), sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess)
         return cleanup(fail(ARTEA_GPU_ENOMEM, "pinned host allocation failed"));
     std::memset(s->h_done, 0, sizeof(uint32_t) * s->ring);
+    *s->h_closed = 0u;
     if (cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_out_alias), s->h_out, 0) != cudaSuccess ||
-        cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_done_alias), s->h_done, 0) != cudaSuccess)
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_done_alias), s->h_done, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_closed_alias), s->h_closed, 0) != cudaSuccess)
         return cleanup(fail(ARTEA_GPU_ECUDA, "mapped host memory unavailable"));
     if (cudaStreamCreateWithFlags(&s->kstream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -432,6 +454,7 @@ extern "C" int artea_gpu_server_destroy(artea_gpu_server* s) {
     if (s->h_meta) cudaFreeHost(s->h_meta);
     if (s->h_out) cudaFreeHost(s->h_out);
     if (s->h_done) cudaFreeHost(s->h_done);
+    if (s->h_closed) cudaFreeHost(s->h_closed);
     if (s->kdone) cudaEventDestroy(s->kdone);
     if (s->kstream) cudaStreamDestroy(s->kstream);
     if (s->cstream) cudaStreamDestroy(s->cstream);

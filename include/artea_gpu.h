@@ -295,7 +295,7 @@ typedef struct artea_gpu_server_opts {
     uint32_t max_queue;      /* largest queue size of any query */
     uint32_t ring_slots;     /* queries in flight (admission limit) */
     uint32_t warps_per_cta;  /* 0 = 2 */
-    uint32_t idle_polls;     /* microseconds idle before the kernel exits; 0 = 5000 */
+    uint32_t idle_polls;     /* microseconds idle before the kernel exits; 0 = 1000000 */
 } artea_gpu_server_opts;
 
 int artea_gpu_server_create(artea_gpu_index* index, const artea_gpu_server_opts* opts, artea_gpu_server** out);
