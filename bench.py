@@ -378,7 +378,15 @@ def run_serving(args, w, base, queries, report, index, device, metric, cache_dir
     points = []
     for rate in rates:
         reqs = make_requests(nq, rate, seed=int(rate))
-        st = run_poisson(srv, qs, reqs, 100)
+        try:
+            st = run_poisson(srv, qs, reqs, 100, timeout_s=120.0)
+        except TimeoutError:
+            # Recorded, not hidden: the rate's requests did not all finish.
+            done = sum(r.n for r in reqs if r.finished is not None)
+            points.append({"offered_qps": rate, "stalled": True, "queries_finished": done, "queries": nq,
+                           "server_stats": srv.stats()})
+            log(f"serving at {rate:.0f} q/s: STALLED after {done} of {nq} queries; later rates skipped")
+            break
         order = sorted(reqs, key=lambda r: r.lo)
         words = np.vstack([r.result for r in order])
         ks = np.concatenate([r.topk for r in order])
