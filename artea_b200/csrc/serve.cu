@@ -291,11 +291,11 @@ extern "C" int artea_gpu_server_create(artea_gpu_index* ix, const artea_gpu_serv
     s->ring = o.ring_slots;
     s->warps = o.warps_per_cta ? o.warps_per_cta : 2;
     if (s->warps > 8) return cleanup(fail(ARTEA_GPU_EINVAL, "warps_per_cta must be <= 8"));
-    // One second by default: a kernel instance that ends and a new one queued
-    // behind it on the same stream has, under relaunches every few
-    // milliseconds, been seen to leave the new one waiting (the old one's warps
-    // had all exited); a long idle window keeps relaunches to quiet periods.
-    s->idle_limit = o.idle_polls ? o.idle_polls : 1000000;   // microseconds
+    // By default the kernel does not end on idle (it ends at destroy): a kernel
+    // instance that ends and a new one queued behind it on the same stream has
+    // been seen to leave the new one waiting although every warp of the old one
+    // had exited. A positive idle_polls restores the idle exit.
+    s->idle_limit = o.idle_polls ? o.idle_polls : 0xFFFFFFFFu;   // microseconds
     s->cap = std::max<uint32_t>(2u * s->qmax, 2u);
     uint32_t kb = 1;
     while (kb < 32 && (1ull << kb) < ix->n) ++kb;

@@ -283,9 +283,11 @@ int artea_gpu_router_tuning(const artea_gpu_router* router, uint32_t* warps_per_
  * copies it in and publishes it to the running kernel, which claims queries
  * one per warp; queries of requests submitted while others run overlap on the
  * device. poll() reports a request done once all its queries are; it copies
- * their rows out and frees the slots. The kernel exits after idle_polls
- * microseconds without work (idle warps read the ring counters without atomics
- * and back off); submit()/poll() relaunch it when work is pending. */
+ * their rows out and frees the slots. Idle warps read the ring counters without
+ * atomics and back off; with idle_polls set the kernel exits after that many
+ * microseconds without work and submit()/poll() relaunch it when work is
+ * pending; by default it stays resident (holding the GPU's warp slots) until
+ * the server is destroyed. */
 typedef struct artea_gpu_server artea_gpu_server;
 
 typedef struct artea_gpu_server_opts {
@@ -295,7 +297,8 @@ typedef struct artea_gpu_server_opts {
     uint32_t max_queue;      /* largest queue size of any query */
     uint32_t ring_slots;     /* queries in flight (admission limit) */
     uint32_t warps_per_cta;  /* 0 = 2 */
-    uint32_t idle_polls;     /* microseconds idle before the kernel exits; 0 = 1000000 */
+    uint32_t idle_polls;     /* microseconds idle before the kernel exits; 0 = never
+                                (the kernel stays resident until destroy) */
 } artea_gpu_server_opts;
 
 int artea_gpu_server_create(artea_gpu_index* index, const artea_gpu_server_opts* opts, artea_gpu_server** out);
