@@ -223,17 +223,64 @@ def cpu_baseline(hgra: str, base: np.ndarray, queries: np.ndarray, topk: int, qu
 
 
 # ---------------------------------------------------------------------------
+def reference_queue(args, w, base, queries, hgra, metric: int):
+    """The queue the GPU arm's sweep settles on: the first of --queues whose
+    recall@k reaches --recall-target, else the largest. EXACT mode returns the
+    reference's words, so the reference's own recall at a queue is the GPU
+    arm's; it is measured here on the first --reference-select queries
+    against the reference's brute force (bruteforce_router_t)."""
+    if args.reference_queue:
+        return args.reference_queue, "given by --reference-queue"
+    from oracle import oracle as orc
+    queues = [int(x) for x in args.queues.split(",") if x]
+    q = queries[: min(args.reference_select, queries.shape[0])]
+    k = w.topk
+    use_ref = orc.have_ref() and host_has_avx512()
+    if use_ref:
+        r = orc.RefRouter(hgra, base)
+        gt = (r.bruteforce(q, k, metric) & np.uint64(0x7FFFFFFF)).astype(np.uint32)
+    else:
+        from artea_b200.graph import CompactHierarchicalGraph
+        g = CompactHierarchicalGraph.from_hgra(hgra)
+        gt = orc.bruteforce(base, q, k, metric=metric)[0]
+    chosen, seen = queues[-1], []
+    for L in queues:
+        if use_ref:
+            words, _ = r.batch_query(q, k, L, metric=metric)
+        else:
+            words = orc.batch_query(g, base, q, k, L, metric=metric, threads=os.cpu_count() or 1)
+        rec = recall(words, gt, k)
+        seen.append(f"{L}: {rec:.4f}")
+        if rec >= args.recall_target:
+            chosen = L
+            break
+    if use_ref:
+        r.close()
+    return chosen, (f"first queue with recall@{k} >= {args.recall_target} on {q.shape[0]} queries against "
+                    f"brute force ({', '.join(seen)})")
+
+
 def run_reference_arm(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     w, base, queries, hgra, report = wl.prepare(args.workload, args.n_base, args.n_query, log=log)
-    queue = args.reference_queue or 200
+    metric = metric_code(w.metric)
     sample = min(args.reference_sample, queries.shape[0])
+    uneven = args.uneven or w.kind == "deep"
+    if uneven:
+        # The GPU arm's uneven batch: per-query topk and queue, same draws.
+        topk, queue = ds.per_query_params(w, queries.shape[0])
+        cfg = {"topk": "per query in {10,100}", "queue": "per query in {64,128,256,512}"}
+        timed = lambda: cpu_baseline_uneven(hgra, base, queries, topk, queue, metric, sample)
+    else:
+        queue, why = reference_queue(args, w, base, queries, hgra, metric)
+        cfg = {"topk": w.topk, "queue": queue, "queue_selection": why}
+        timed = lambda: cpu_baseline(hgra, base, queries, w.topk, queue, metric, sample)
     vals = []
     info = None
     for i in range(args.warmup + args.steps):
-        info = cpu_baseline(hgra, base, queries, w.topk, queue, metric_code(w.metric), sample)
+        info = timed()
         if i >= args.warmup:
             vals.append(info["value"])
     value = statistics.mean(vals)
@@ -241,7 +288,7 @@ def run_reference_arm(args) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sample / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": {"workload": w.name, "n_base": w.n_base, "n_query": sample,
-                                           "dim": w.dim, "metric": w.metric, "topk": w.topk, "queue": queue},
+                                           "dim": w.dim, "metric": w.metric, **cfg},
             "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -437,6 +484,8 @@ def main() -> None:
     ap.add_argument("--no-graphs", action="store_true", help="launch directly instead of replaying CUDA graphs")
     ap.add_argument("--reference-queue", type=int, default=0)
     ap.add_argument("--reference-sample", type=int, default=2000)
+    ap.add_argument("--reference-select", type=int, default=200,
+                    help="queries on which the reference arm measures recall to pick its queue")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: one warm and one measured launch at --profile-queue with "
                          "--profile-warps warps per CTA; no sweep, ground truth or baseline")
