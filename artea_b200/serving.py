@@ -114,12 +114,23 @@ def make_requests(nq_total: int, rate_qps: float, seed: int, topk_choices=(10, 1
     return reqs
 
 
+def latency_percentile(lat, p: float) -> float:
+    """The reference profiler's pick (router/profiler/hg_router_profiler.hpp:429-444):
+    the sorted sample at index floor(n * p), clamped to the last one; no
+    interpolation."""
+    s = np.sort(np.asarray(lat, dtype=np.float64))
+    if s.size == 0:
+        return float("nan")
+    return float(s[min(int(s.size * p), s.size - 1)])
+
+
 def _summarise(reqs: List[Request], wall: float) -> dict:
     lat = np.array([(r.finished - r.arrival) * 1e3 for r in reqs])
     nq = sum(r.n for r in reqs)
     return {"requests": len(reqs), "queries": nq, "qps": nq / wall, "wall_s": wall,
-            "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
-            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean())}
+            "p50_ms": latency_percentile(lat, 0.50), "p90_ms": latency_percentile(lat, 0.90),
+            "p95_ms": latency_percentile(lat, 0.95), "p99_ms": latency_percentile(lat, 0.99),
+            "mean_ms": float(lat.mean())}
 
 
 def run_poisson(server: Server, queries: np.ndarray, reqs: List[Request], k_stride: int,

@@ -145,3 +145,16 @@ def test_null_arguments_are_rejected():
     assert L.artea_gpu_router_destroy(None) == nat.OK
     assert L.artea_gpu_index_destroy(None) == nat.OK
     assert L.artea_gpu_batch_query(None, None, 0, None, None, 0, None, None) == nat.EINVAL
+
+
+def test_serving_percentiles_use_the_reference_profilers_pick():
+    # hg_router_profiler.hpp:429-444: sorted[floor(n * p)], clamped; no interpolation.
+    from artea_b200.serving import latency_percentile
+    lat = [5.0, 1.0, 4.0, 2.0, 3.0]
+    assert latency_percentile(lat, 0.50) == 3.0       # index 2
+    assert latency_percentile(lat, 0.90) == 5.0       # index 4
+    assert latency_percentile(lat, 0.99) == 5.0
+    assert latency_percentile(list(range(100)), 0.99) == 99.0
+    assert latency_percentile(list(range(100)), 0.95) == 95.0
+    assert latency_percentile([7.0], 0.5) == 7.0
+    assert np.isnan(latency_percentile([], 0.5))
