@@ -106,6 +106,7 @@ SIGNATURES = {
     "artea_gpu_graph_validate": (c_int, [POINTER(GraphDesc)]),
     "artea_gpu_index_create": (c_int, [POINTER(GraphDesc), c_void_p, c_uint32, c_uint32, c_int, POINTER(c_void_p)]),
     "artea_gpu_index_create_from_hgra": (c_int, [c_char_p, c_void_p, c_uint32, c_uint32, c_int, POINTER(c_void_p)]),
+    "artea_gpu_index_download": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "artea_gpu_index_destroy": (c_int, [c_void_p]),
     "artea_gpu_index_bytes": (c_int, [c_void_p, POINTER(c_uint64)]),
     "artea_gpu_router_create": (c_int, [c_void_p, c_uint32, c_uint32, POINTER(RouterOpts), POINTER(c_void_p)]),

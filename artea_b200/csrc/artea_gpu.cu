@@ -510,6 +510,72 @@ int run_device(artea_gpu_router* r, const float* d_q, uint32_t nq, const uint32_
 
 }  // namespace
 
+namespace artea_gpu {
+
+int index_begin(uint32_t num_vertices, const float* vectors, uint32_t num_vectors, uint32_t dim, int device,
+                artea_gpu_index** out) {
+    *out = nullptr;
+    if (dim == 0 || dim % 16 != 0) return fail(ARTEA_GPU_EINVAL, "dim must be a positive multiple of 16");
+    if (num_vectors < num_vertices) return fail(ARTEA_GPU_EINVAL, "fewer vectors than graph vertices");
+    if (num_vectors && !vectors) return fail(ARTEA_GPU_EINVAL, "null vectors");
+    int ndev = 0;
+    if (artea_gpu_device_count(&ndev) != ARTEA_GPU_OK || device < 0 || device >= ndev)
+        return fail(ARTEA_GPU_ENODEV, "CUDA device " + std::to_string(device) + " not available");
+    DeviceGuard guard(device);
+    auto* ix = new artea_gpu_index();
+    ix->device = device;
+    ix->dim = dim;
+    ix->nvecs = num_vectors;
+    const size_t nvec = static_cast<size_t>(std::max(num_vectors, 1u)) * dim;
+    if (int rc = dev_alloc(&ix->d_vecs, nvec)) {
+        artea_gpu_index_destroy(ix);
+        return rc;
+    }
+    if (num_vectors && cudaMemcpy(ix->d_vecs, vectors, sizeof(float) * static_cast<size_t>(num_vectors) * dim,
+                                  cudaMemcpyHostToDevice) != cudaSuccess) {
+        artea_gpu_index_destroy(ix);
+        return fail(ARTEA_GPU_ECUDA, "vector upload failed");
+    }
+    ix->bytes += sizeof(float) * nvec;
+    *out = ix;
+    return ARTEA_GPU_OK;
+}
+
+int index_finish_l0(artea_gpu_index* ix, const uint32_t* vertex_info, const uint64_t* const* group_offsets) {
+    // Level-0 row descriptors (start | length << 40), one load per expansion.
+    if (ix->n_nbrs >= (1ull << kRowLenShift) || ix->bl >= (1u << 24))
+        return fail(ARTEA_GPU_EGRAPH, "graph too large for 40-bit row offsets");
+    std::vector<unsigned long long> l0row(ix->n, 0ull);
+    for (uint32_t v = 0; v < ix->n; ++v) {
+        const uint32_t hl = vertex_info[2 * v];
+        if (hl == kInvalidLevel) continue;
+        const uint64_t local = vertex_info[2 * v + 1];
+        const uint64_t rrow = local * (hl + 1ull) + hl;
+        const uint64_t b = group_offsets[hl][rrow], e = group_offsets[hl][rrow + 1];
+        l0row[v] = b | ((e - b) << kRowLenShift);
+    }
+    if (int rc = dev_alloc(&ix->d_l0row, ix->n)) return rc;
+    if (cudaMemcpy(ix->d_l0row, l0row.data(), sizeof(unsigned long long) * ix->n, cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+        return fail(ARTEA_GPU_ECUDA, "row descriptor upload failed");
+    ix->bytes += sizeof(uint2) * ix->n + sizeof(uint32_t) * std::max<uint64_t>(ix->n_nbrs, 1) +
+                 sizeof(uint64_t) * ix->n_offsets + sizeof(unsigned long long) * ix->n;
+    int* d_repeat = nullptr;
+    if (int rc = dev_alloc(&d_repeat, 1)) return rc;
+    int repeat = 1;
+    cudaMemset(d_repeat, 0, sizeof(int));
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
+    l0_rows_repeat_kernel<<<std::max(sms, 1) * 8, 256>>>(ix->d_l0row, ix->d_nbrs, ix->n, d_repeat);
+    const cudaError_t e = cudaMemcpy(&repeat, d_repeat, sizeof(int), cudaMemcpyDeviceToHost);
+    dev_free(d_repeat);
+    if (e != cudaSuccess) return fail(ARTEA_GPU_ECUDA, "row check failed");
+    ix->l0_unique = repeat ? 0u : 1u;
+    return ARTEA_GPU_OK;
+}
+
+}  // namespace artea_gpu
+
 extern "C" {
 
 const char* artea_gpu_version(void) { return "artea-b200 0.1 (sm_100a)"; }
@@ -536,16 +602,10 @@ int artea_gpu_index_create(const artea_gpu_graph_desc* g, const float* vectors, 
     if (num_vectors < g->num_vertices) return fail(ARTEA_GPU_EINVAL, "fewer vectors than graph vertices");
     if (num_vectors && !vectors) return fail(ARTEA_GPU_EINVAL, "null vectors");
     if (int rc = artea_gpu_graph_validate(g)) return rc;
-    int ndev = 0;
-    if (artea_gpu_device_count(&ndev) != ARTEA_GPU_OK || device < 0 || device >= ndev)
-        return fail(ARTEA_GPU_ENODEV, "CUDA device " + std::to_string(device) + " not available");
+    artea_gpu_index* ix = nullptr;
+    if (int rc = artea_gpu::index_begin(g->num_vertices, vectors, num_vectors, dim, device, &ix)) return rc;
     DeviceGuard guard(device);
-
-    auto* ix = new artea_gpu_index();
-    ix->device = device;
     ix->n = g->num_vertices;
-    ix->dim = dim;
-    ix->nvecs = num_vectors;
     const bool empty = g->num_vertices == 0 || g->top_level == kInvalidLevel;
     ix->top = empty ? kInvalidLevel : g->top_level;
     ix->entry = g->entry_point_vid;
@@ -555,18 +615,11 @@ int artea_gpu_index_create(const artea_gpu_graph_desc* g, const float* vectors, 
         artea_gpu_index_destroy(ix);
         return rc;
     };
-    const size_t nvec = static_cast<size_t>(std::max(num_vectors, 1u)) * dim;
-    if (int rc = dev_alloc(&ix->d_vecs, nvec)) return cleanup(rc);
-    if (num_vectors) {
-        if (cudaMemcpy(ix->d_vecs, vectors, sizeof(float) * static_cast<size_t>(num_vectors) * dim,
-                       cudaMemcpyHostToDevice) != cudaSuccess)
-            return cleanup(fail(ARTEA_GPU_ECUDA, "vector upload failed"));
-    }
-    ix->bytes += sizeof(float) * nvec;
     if (!empty) {
         if (int rc = dev_alloc(&ix->d_vinfo, ix->n)) return cleanup(rc);
         if (cudaMemcpy(ix->d_vinfo, g->vertex_info, sizeof(uint2) * ix->n, cudaMemcpyHostToDevice) != cudaSuccess)
             return cleanup(fail(ARTEA_GPU_ECUDA, "vertex table upload failed"));
+        ix->n_nbrs = g->num_neighbor_ids;
         const uint64_t nn = std::max<uint64_t>(g->num_neighbor_ids, 1);
         if (int rc = dev_alloc(&ix->d_nbrs, nn)) return cleanup(rc);
         if (g->num_neighbor_ids &&
@@ -575,6 +628,7 @@ int artea_gpu_index_create(const artea_gpu_graph_desc* g, const float* vectors, 
             return cleanup(fail(ARTEA_GPU_ECUDA, "neighbour upload failed"));
         uint64_t total = 0;
         for (uint32_t h = 0; h <= ix->top; ++h) total += g->group_sizes[h] * (h + 1ull) + 1;
+        ix->n_offsets = total;
         if (int rc = dev_alloc(&ix->d_offsets, total)) return cleanup(rc);
         uint64_t at = 0;
         for (uint32_t h = 0; h <= ix->top; ++h) {
@@ -585,67 +639,10 @@ int artea_gpu_index_create(const artea_gpu_graph_desc* g, const float* vectors, 
             ix->group_ptr[h] = ix->d_offsets + at;
             at += cnt;
         }
-        // Level-0 row descriptors (start | length << 40), one load per expansion.
-        if (g->num_neighbor_ids >= (1ull << kRowLenShift) || g->bl_max_nbr_size >= (1u << 24))
-            return cleanup(fail(ARTEA_GPU_EGRAPH, "graph too large for 40-bit row offsets"));
-        std::vector<unsigned long long> l0row(ix->n, 0ull);
-        for (uint32_t v = 0; v < ix->n; ++v) {
-            const uint32_t hl = g->vertex_info[2 * v];
-            if (hl == kInvalidLevel) continue;
-            const uint64_t local = g->vertex_info[2 * v + 1];
-            const uint64_t rrow = local * (hl + 1ull) + hl;
-            const uint64_t b = g->group_offsets[hl][rrow], e = g->group_offsets[hl][rrow + 1];
-            l0row[v] = b | ((e - b) << kRowLenShift);
-        }
-        if (int rc = dev_alloc(&ix->d_l0row, ix->n)) return cleanup(rc);
-        if (cudaMemcpy(ix->d_l0row, l0row.data(), sizeof(unsigned long long) * ix->n, cudaMemcpyHostToDevice) !=
-            cudaSuccess)
-            return cleanup(fail(ARTEA_GPU_ECUDA, "row descriptor upload failed"));
-        ix->bytes += sizeof(uint2) * ix->n + sizeof(uint32_t) * nn + sizeof(uint64_t) * total +
-                     sizeof(unsigned long long) * ix->n;
-        int* d_repeat = nullptr;
-        if (int rc = dev_alloc(&d_repeat, 1)) return cleanup(rc);
-        int repeat = 1;
-        cudaMemset(d_repeat, 0, sizeof(int));
-        int sms = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        artea_gpu::l0_rows_repeat_kernel<<<std::max(sms, 1) * 8, 256>>>(ix->d_l0row, ix->d_nbrs, ix->n, d_repeat);
-        const cudaError_t e = cudaMemcpy(&repeat, d_repeat, sizeof(int), cudaMemcpyDeviceToHost);
-        dev_free(d_repeat);
-        if (e != cudaSuccess) return cleanup(fail(ARTEA_GPU_ECUDA, "row check failed"));
-        ix->l0_unique = repeat ? 0u : 1u;
+        if (int rc = artea_gpu::index_finish_l0(ix, g->vertex_info, g->group_offsets)) return cleanup(rc);
     }
     *out = ix;
     return ARTEA_GPU_OK;
-}
-
-int artea_gpu_index_create_from_hgra(const char* path, const float* vectors, uint32_t num_vectors, uint32_t dim,
-                                     int device, artea_gpu_index** out) {
-    if (!path || !out) return fail(ARTEA_GPU_EINVAL, "null argument");
-    artea_gpu_hgra_info info;
-    if (int rc = artea_gpu_hgra_probe(path, &info)) return rc;
-    std::vector<uint32_t> vinfo(2ull * info.num_vertices);
-    std::vector<uint64_t> offsets(info.num_offsets);
-    std::vector<uint32_t> nbrs(std::max<uint64_t>(info.num_neighbor_ids, 1));
-    if (int rc = artea_gpu_hgra_read(path, vinfo.data(), offsets.data(), nbrs.data())) return rc;
-    std::vector<const uint64_t*> gptr(info.num_groups);
-    uint64_t at = 0;
-    for (uint32_t h = 0; h < info.num_groups; ++h) {
-        gptr[h] = offsets.data() + at;
-        at += info.group_sizes[h] * (h + 1ull) + 1;
-    }
-    artea_gpu_graph_desc g;
-    g.num_vertices = info.num_vertices;
-    g.top_level = info.num_vertices == 0 ? kInvalidLevel : info.top_level;
-    g.ul_max_nbr_size = info.ul_max_nbr_size;
-    g.bl_max_nbr_size = info.bl_max_nbr_size;
-    g.entry_point_vid = info.entry_point_vid;
-    g.vertex_info = vinfo.data();
-    g.group_offsets = gptr.data();
-    g.group_sizes = info.group_sizes;
-    g.neighbor_ids = nbrs.data();
-    g.num_neighbor_ids = info.num_neighbor_ids;
-    return artea_gpu_index_create(&g, vectors, num_vectors, dim, device, out);
 }
 
 int artea_gpu_index_destroy(artea_gpu_index* ix) {

@@ -31,6 +31,8 @@ struct artea_gpu_index {
     uint64_t* d_offsets = nullptr;
     unsigned long long* d_l0row = nullptr;
     const uint64_t* group_ptr[artea_gpu::kMaxGroups] = {};
+    uint64_t n_offsets = 0;   // entries of d_offsets (all groups, with their end sentinels)
+    uint64_t n_nbrs = 0;      // entries of d_nbrs in use
     uint64_t bytes = 0;
 };
 
@@ -67,5 +69,15 @@ inline void dev_free(T*& p) {
     if (p) cudaFree(p);
     p = nullptr;
 }
+
+// Steps of index creation shared by the host-graph and the snapshot paths
+// (artea_gpu.cu).
+// Checks dim / vector count / device and uploads the vectors into a new index.
+int index_begin(uint32_t num_vertices, const float* vectors, uint32_t num_vectors, uint32_t dim, int device,
+                artea_gpu_index** out);
+// With d_vinfo, d_nbrs and d_offsets in place (group h's offsets at
+// group_offsets_host[h] on the host): the level-0 row descriptors and the
+// row-repeat check.
+int index_finish_l0(artea_gpu_index* ix, const uint32_t* vertex_info, const uint64_t* const* group_offsets_host);
 
 }  // namespace artea_gpu

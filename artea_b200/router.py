@@ -90,6 +90,16 @@ class DeviceIndex:
             raise RuntimeError("index is closed")
         return self._h
 
+    def download_graph(self, num_vertices: int, num_offsets: int, num_neighbor_ids: int):
+        """The device graph as (vertex_info (n, 2) uint32, offsets (all groups
+        concatenated) uint64, neighbor_ids uint32), sized as artea_gpu_hgra_probe
+        reports them (artea_gpu_index_download)."""
+        vinfo = np.empty((num_vertices, 2), dtype=np.uint32)
+        offs = np.empty(num_offsets, dtype=np.uint64)
+        nbrs = np.empty(max(num_neighbor_ids, 1), dtype=np.uint32)
+        nat.check(nat.lib().artea_gpu_index_download(self.handle, nat.ptr(vinfo), nat.ptr(offs), nat.ptr(nbrs)))
+        return vinfo, offs, nbrs[:num_neighbor_ids]
+
     def nbytes(self) -> int:
         b = ctypes.c_uint64()
         nat.check(nat.lib().artea_gpu_index_bytes(self.handle, ctypes.byref(b)))

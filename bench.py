@@ -468,6 +468,66 @@ def run_serving(args, w, base, queries, report, index, device, metric, cache_dir
     print(json.dumps(line), flush=True)
 
 
+def run_restore(args, w, base, hgra, device):
+    """HGRA snapshot -> searchable device index: the streamed device restore
+    (artea_gpu_index_create_from_hgra) against the host reader + upload
+    (artea_gpu_hgra_read + artea_gpu_index_create) and the reference's
+    HierarchicalGraphFileManager::restore on the host cores. The file is in the
+    page cache for every timing; vector uploads are timed alone and reported
+    apart, since the reference's restore reads no vectors."""
+    import torch
+    from artea_b200.graph import CompactHierarchicalGraph
+    from artea_b200.router import DeviceIndex, vectors_only_graph
+    from oracle import oracle as orc
+    with open(hgra, "rb") as f:
+        while f.read(1 << 26):
+            pass
+    reps = max(1, min(args.steps, 5))
+
+    def timed(make):
+        out = []
+        for i in range(1 + reps):
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            ix = make()
+            torch.cuda.synchronize(device)
+            dt = time.perf_counter() - t0
+            ix.close()
+            if i:
+                out.append(dt)
+        return statistics.median(out)
+
+    dev = local_gpu(device)
+    t_stream = timed(lambda: DeviceIndex.from_hgra(hgra, base, device=dev))
+    t_host = timed(lambda: DeviceIndex(CompactHierarchicalGraph.from_hgra(hgra), base, device=dev))
+    t_vec = timed(lambda: DeviceIndex(vectors_only_graph(), base, device=dev))
+    # What is timed is checked: the streamed device graph equals the host reader's.
+    g = CompactHierarchicalGraph.from_hgra(hgra)
+    ix = DeviceIndex.from_hgra(hgra, base, device=dev)
+    offs = np.concatenate(g.group_offsets)
+    vi, of, nb = ix.download_graph(g.num_vertices, offs.size, g.neighbor_ids.size)
+    same = bool(np.array_equal(vi, g.vertex_info) and np.array_equal(of, offs) and np.array_equal(nb, g.neighbor_ids))
+    ix.close()
+    assert same, "streamed restore differs from the host reader"
+    ref_s, ref_kind = None, None
+    if orc.have_ref():
+        orc.ref_restore_seconds(hgra)
+        ref_s = statistics.median([orc.ref_restore_seconds(hgra) for _ in range(reps)])
+        ref_kind = "reference"
+    size = os.path.getsize(hgra)
+    line = {"metric": "HGRA snapshot restore to a searchable device index", "value": t_stream, "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "steps": reps, "warmup": 1, "data": "synthetic", "dtype": "u32",
+            "config": {"workload": w.name, "n_base": w.n_base, "dim": w.dim, "snapshot_bytes": size,
+                       "graph_levels": g.group_sizes().tolist(), "page_cache": "warm"},
+            "streamed_restore_s": t_stream, "host_reader_then_upload_s": t_host, "vectors_only_s": t_vec,
+            "graph_part_streamed_s": t_stream - t_vec, "graph_part_host_s": t_host - t_vec,
+            "snapshot_gbs_streamed": size / max(t_stream - t_vec, 1e-9) / 1e9,
+            "reference_restore_s": ref_s, "reference_kind": ref_kind,
+            "reference_threads": int(orc.ref_lib().artea_ref_max_threads()) if ref_s is not None else None,
+            "device_graph_equals_host_reader": same}
+    print(json.dumps(line), flush=True)
+
+
 def local_gpu(device) -> int:
     return device.index if getattr(device, "index", None) is not None else 0
 
@@ -507,6 +567,9 @@ def main() -> None:
     ap.add_argument("--serve", action="store_true",
                     help="serving loop under Poisson arrivals (request sizes log-uniform in [1,256], topk in "
                          "{10,100}, queue in {100,200,400}) against one batch_query launch per request")
+    ap.add_argument("--restore", action="store_true",
+                    help="HGRA snapshot to device index: streamed restore vs host reader + upload vs the reference's "
+                         "restore")
     ap.add_argument("--serve-rates", default="1000,10000,50000,100000,200000")
     ap.add_argument("--serve-queries", type=int, default=20000)
     args = ap.parse_args()
@@ -533,6 +596,9 @@ def main() -> None:
     torch.cuda.set_device(device)
 
     w, base, queries, hgra, report = wl.prepare(args.workload, args.n_base, args.n_query, log=log)
+    if args.restore:
+        run_restore(args, w, base, hgra, device)
+        return
     metric = metric_code(w.metric)
     nq, dim, k = queries.shape[0], base.shape[1], w.topk
     graph = CompactHierarchicalGraph.from_hgra(hgra)

@@ -176,9 +176,22 @@ int artea_gpu_graph_validate(const artea_gpu_graph_desc* graph);
  * multiple of 16, rows padded with zeros as the reference pads them). */
 int artea_gpu_index_create(const artea_gpu_graph_desc* graph, const float* vectors, uint32_t num_vectors,
                            uint32_t dim, int device, artea_gpu_index** out);
-/* Same, reading the graph from an HGRA v1 snapshot. */
+/* Same, restoring the graph from an HGRA v1 snapshot straight to the device;
+ * replaces HierarchicalGraphFileManager::restore
+ * (index/persistence/hierarchical_graph_file_manager.hpp:152-300) followed by
+ * an upload. The file streams through pinned buffers into device memory while
+ * the host reads only the record headers; the ids are moved into the compact
+ * graph's CSR layout and checked on the device. Same layout, same accepted
+ * files and same status codes as artea_gpu_hgra_read + artea_gpu_index_create
+ * (EIO for what the reader rejects, EGRAPH for what validation rejects). */
 int artea_gpu_index_create_from_hgra(const char* path, const float* vectors, uint32_t num_vectors,
                                      uint32_t dim, int device, artea_gpu_index** out);
+/* Copies the device graph back into caller buffers sized as for
+ * artea_gpu_hgra_read (vertex_info 2*num_vertices u32, offsets num_offsets
+ * u64, neighbor_ids num_neighbor_ids u32); with artea_gpu_hgra_write it
+ * snapshots a device index. EINVAL for an index without a graph. */
+int artea_gpu_index_download(const artea_gpu_index* index, uint32_t* vertex_info, uint64_t* offsets,
+                             uint32_t* neighbor_ids);
 int artea_gpu_index_destroy(artea_gpu_index* index);
 /* Device bytes held by the index (vectors + CSR). */
 int artea_gpu_index_bytes(const artea_gpu_index* index, uint64_t* bytes);

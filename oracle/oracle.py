@@ -92,6 +92,8 @@ def ref_lib():
         L.artea_ref_distance.restype = c_float
         L.artea_ref_distance.argtypes = [c_int, c_void_p, c_void_p, c_uint32]
         L.artea_ref_max_threads.restype = c_int
+        L.artea_ref_restore_seconds.restype = ctypes.c_longlong
+        L.artea_ref_restore_seconds.argtypes = [c_char_p, POINTER(c_double)]
         _rlib = L
     return _rlib
 
@@ -110,6 +112,15 @@ def ref_distance(metric: int, a: np.ndarray, b: np.ndarray) -> float:
     a = np.ascontiguousarray(a, dtype=np.float32)
     b = np.ascontiguousarray(b, dtype=np.float32)
     return float(ref_lib().artea_ref_distance(metric, _p(a), _p(b), a.size))
+
+
+def ref_restore_seconds(hgra_path: str) -> float:
+    """The reference's HierarchicalGraphFileManager::restore of a snapshot, timed."""
+    secs = c_double()
+    n = ref_lib().artea_ref_restore_seconds(os.fsencode(hgra_path), ctypes.byref(secs))
+    if n < 0:
+        raise RuntimeError(ref_lib().artea_ref_last_error().decode())
+    return secs.value
 
 
 class EarlyStopNotRepresentable(OverflowError):

@@ -203,6 +203,22 @@ void* artea_ref_open(const char* hgra_path, const float* vecs, uint32_t n, uint3
 
 void artea_ref_close(void* h) { delete static_cast<RefIndex*>(h); }
 
+// Seconds taken by hierarchical_graph_file_manager_t::restore of the
+// snapshot alone (index/persistence/hierarchical_graph_file_manager.hpp:152),
+// the reference's way from an HGRA file to a searchable compact graph; the
+// number of vertices restored, or -1 on an error.
+long long artea_ref_restore_seconds(const char* hgra_path, double* seconds) {
+    try {
+        const auto t0 = std::chrono::steady_clock::now();
+        auto g = hierarchical_graph_file_manager_t::restore(hgra_path);
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return static_cast<long long>(g.get_num_vertices());
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
 // metric: 0 EUCLIDEAN_SQR, 1 EUCLIDEAN, 2 COSINE, 3 DOT. out: nq*topk words.
 // threads > 0 caps the worker count (tbb::global_control); dist_calls, if not
 // null, switches to sequential per-query calls with a counting distance.
