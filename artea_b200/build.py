@@ -29,7 +29,7 @@ REF = os.environ.get("ARTEA_REFERENCE", "/root/reference")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-pthread",
     "-shared",
 ]
 

@@ -14,10 +14,19 @@
 // and checks them, so the ids cross the host once (the file read) and are
 // never parsed there. Layout, accepted files and status codes are those of
 // artea_gpu_hgra_read followed by artea_gpu_index_create.
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
-#include <cstdio>
+#include <cerrno>
+#include <condition_variable>
 #include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -29,37 +38,54 @@ namespace {
 constexpr uint32_t kMagic = 0x48475241u;
 constexpr uint32_t kVersion = 1u;
 constexpr uint32_t kNone = 0xffffffffu;
-constexpr size_t kChunkWords = size_t(1) << 23;   // 32 MiB per pinned buffer
+constexpr size_t kChunkWords = size_t(1) << 22;   // 16 MiB per pinned buffer
+constexpr int kReaders = 4;                         // reader threads, one pinned buffer each
+constexpr uint64_t kFree = ~0ull;
 
 constexpr uint32_t kFlagBadId = 1u;      // an id >= num_vertices (the reader's EIO)
 constexpr uint32_t kFlagOffLevel = 2u;   // an id whose vertex is not on the row's level (validation's EGRAPH)
 
+constexpr uint32_t kGroupsMax = 64;
+
+// The CSR's row groups: group h holds the flattened rows [row_begin[h],
+// row_begin[h + 1]) and its offsets start at offsets + obase[h].
+struct RowGroups {
+    unsigned long long row_begin[kGroupsMax + 1];
+    unsigned long long obase[kGroupsMax];
+    uint32_t groups;
+};
+
 // One warp per CSR row (grid-stride): copies the row's ids from the raw
 // records to their CSR position and flags ids out of range or off the row's
-// level. src/dst/len come from the host's header walk, which checked that
-// every row lies inside the raw copy and inside the CSR array.
+// level. A row's destination and length come from the CSR offsets, its level
+// from its position in the group, its source from src (the host's header walk
+// checked that every row lies inside the raw copy).
 __global__ void hgra_rows_kernel(const uint32_t* __restrict__ raw, const unsigned long long* __restrict__ src,
-                                 const unsigned long long* __restrict__ dst,
-                                 const unsigned long long* __restrict__ len_lvl, unsigned long long rows,
+                                 RowGroups gr, const uint64_t* __restrict__ offsets,
                                  const uint2* __restrict__ vinfo, uint32_t n, uint32_t* __restrict__ nbrs,
                                  uint32_t* flags) {
     const int lane = threadIdx.x & 31;
     const unsigned long long wpb = blockDim.x >> 5;
     const unsigned long long warps = static_cast<unsigned long long>(gridDim.x) * wpb;
+    const unsigned long long rows = gr.row_begin[gr.groups];
     uint32_t bad = 0;
+    uint32_t h = 0;   // the warp's rows only grow, so its group index only moves forward
     for (unsigned long long r = blockIdx.x * wpb + (threadIdx.x >> 5); r < rows; r += warps) {
-        const unsigned long long m = len_lvl[r];
-        const uint32_t len = static_cast<uint32_t>(m);
-        const uint32_t lvl = static_cast<uint32_t>(m >> 32);
-        const unsigned long long s = src[r], d = dst[r];
+        while (r >= gr.row_begin[h + 1]) ++h;
+        const unsigned long long rr = r - gr.row_begin[h];
+        const uint64_t* o = offsets + gr.obase[h];
+        const unsigned long long d = o[rr];
+        const uint32_t len = static_cast<uint32_t>(o[rr + 1] - d);
+        const uint32_t lvl = h - static_cast<uint32_t>(rr % (h + 1ull));
+        const unsigned long long s = src[r];
         for (uint32_t i = lane; i < len; i += 32) {
             const uint32_t id = raw[s + i];
             nbrs[d + i] = id;
             if (id >= n) {
                 bad |= kFlagBadId;
             } else {
-                const uint32_t h = vinfo[id].x;
-                if (h == kNone || h < lvl) bad |= kFlagOffLevel;
+                const uint32_t vh = vinfo[id].x;
+                if (vh == kNone || vh < lvl) bad |= kFlagOffLevel;
             }
         }
     }
@@ -69,36 +95,88 @@ __global__ void hgra_rows_kernel(const uint32_t* __restrict__ raw, const unsigne
 
 // Host resources of one restore; released on every exit path.
 struct Restore {
-    FILE* fp = nullptr;
+    int fd = -1;
     cudaStream_t stream = nullptr;
-    uint32_t* pinned[2] = {nullptr, nullptr};
-    cudaEvent_t copied[2] = {nullptr, nullptr};
+    uint32_t* pinned[kReaders] = {};
+    cudaEvent_t copied[kReaders] = {};
     uint32_t* d_raw = nullptr;
     unsigned long long* d_src = nullptr;
-    unsigned long long* d_dst = nullptr;
-    unsigned long long* d_len = nullptr;
     uint32_t* d_flags = nullptr;
     int device = -1;   // set once device resources exist
+    // Reader t fills buffer t with chunks t, t + kReaders, ... in order, each
+    // once the walk has released the buffer (holds[t] == kFree).
+    std::vector<std::thread> readers;
+    std::mutex mu;
+    std::condition_variable cv;
+    uint64_t holds[kReaders];
+    bool read_ok[kReaders] = {};
+    bool stop = false;
+
+    Restore() {
+        for (auto& h : holds) h = kFree;
+    }
+
+    void stop_readers() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        cv.notify_all();
+        for (auto& t : readers)
+            if (t.joinable()) t.join();
+        readers.clear();
+    }
     ~Restore() {
-        if (device < 0) {
-            if (fp) std::fclose(fp);
-            return;
+        stop_readers();
+        if (device >= 0) {
+            DeviceGuard guard(device);
+            if (stream) cudaStreamSynchronize(stream);
+            for (int i = 0; i < kReaders; ++i) {
+                if (pinned[i]) cudaFreeHost(pinned[i]);
+                if (copied[i]) cudaEventDestroy(copied[i]);
+            }
+            dev_free(d_raw);
+            dev_free(d_src);
+            dev_free(d_flags);
+            if (stream) cudaStreamDestroy(stream);
         }
-        DeviceGuard guard(device);
-        if (stream) cudaStreamSynchronize(stream);
-        if (fp) std::fclose(fp);
-        for (int i = 0; i < 2; ++i) {
-            if (pinned[i]) cudaFreeHost(pinned[i]);
-            if (copied[i]) cudaEventDestroy(copied[i]);
-        }
-        dev_free(d_raw);
-        dev_free(d_src);
-        dev_free(d_dst);
-        dev_free(d_len);
-        dev_free(d_flags);
-        if (stream) cudaStreamDestroy(stream);
+        if (fd >= 0) close(fd);
     }
 };
+
+bool pread_all(int fd, void* dst, size_t bytes, off_t at) {
+    char* p = static_cast<char*>(dst);
+    while (bytes) {
+        const ssize_t k = pread(fd, p, bytes, at);
+        if (k < 0 && errno == EINTR) continue;
+        if (k <= 0) return false;
+        p += k;
+        bytes -= static_cast<size_t>(k);
+        at += k;
+    }
+    return true;
+}
+
+// Reader thread t: chunks t, t + kReaders, ... of the records (which start
+// after the 28-byte header) into pinned buffer t.
+void read_chunks(Restore* rs, int t, uint64_t nchunks, uint64_t rec_words) {
+    for (uint64_t c = static_cast<uint64_t>(t); c < nchunks; c += kReaders) {
+        {
+            std::unique_lock<std::mutex> lk(rs->mu);
+            rs->cv.wait(lk, [&] { return rs->stop || rs->holds[t] == kFree; });
+            if (rs->stop) return;
+        }
+        const uint64_t off = c * kChunkWords;
+        const size_t bytes = static_cast<size_t>(std::min<uint64_t>(kChunkWords, rec_words - off)) * 4;
+        const bool ok = pread_all(rs->fd, rs->pinned[t], bytes, static_cast<off_t>(28 + off * 4));
+        {
+            std::lock_guard<std::mutex> lk(rs->mu);
+            rs->holds[t] = c;
+            rs->read_ok[t] = ok;
+        }
+        rs->cv.notify_all();
+    }
+}
 
 }  // namespace
 
@@ -115,21 +193,21 @@ extern "C" int artea_gpu_index_create_from_hgra(const char* path, const float* v
     if (!path || !out) return fail(ARTEA_GPU_EINVAL, "null argument");
     *out = nullptr;
     Restore rs;
-    rs.fp = std::fopen(path, "rb");
-    if (!rs.fp) return fail(ARTEA_GPU_EIO, std::string("cannot open ") + path);
-    std::fseek(rs.fp, 0, SEEK_END);
-    const long bytes = std::ftell(rs.fp);
-    std::fseek(rs.fp, 0, SEEK_SET);
+    rs.fd = open(path, O_RDONLY | O_CLOEXEC);
+    if (rs.fd < 0) return fail(ARTEA_GPU_EIO, std::string("cannot open ") + path);
+    struct stat st;
+    if (fstat(rs.fd, &st) != 0) return fail(ARTEA_GPU_EIO, std::string("cannot stat ") + path);
+    const uint64_t bytes = static_cast<uint64_t>(st.st_size);
     if (bytes < 28 || bytes % 4 != 0)
         return fail(ARTEA_GPU_EIO, std::string("truncated or misaligned snapshot ") + path);
     uint32_t hdr[7];
-    if (std::fread(hdr, 4, 7, rs.fp) != 7) return fail(ARTEA_GPU_EIO, std::string("short read of ") + path);
+    if (!pread_all(rs.fd, hdr, sizeof(hdr), 0)) return fail(ARTEA_GPU_EIO, std::string("short read of ") + path);
     if (hdr[0] != kMagic) return fail(ARTEA_GPU_EIO, "bad HGRA magic");
     if (hdr[1] != kVersion) return fail(ARTEA_GPU_EIO, "unsupported HGRA version");
     const uint32_t n = hdr[2], top = hdr[3], ul = hdr[4], bl = hdr[5], entry = hdr[6];
     if (top == kNone || (entry != kNone && entry >= n && n != 0)) return fail(ARTEA_GPU_EIO, "invalid HGRA header");
     if (top >= 64) return fail(ARTEA_GPU_EIO, "HGRA top level above 63 is not supported");
-    const uint64_t rec_words = static_cast<uint64_t>(bytes) / 4 - 7;
+    const uint64_t rec_words = bytes / 4 - 7;
     // Every vertex record holds at least its highest-level word.
     if (rec_words < n) return fail(ARTEA_GPU_EIO, "HGRA truncated at vid " + std::to_string(rec_words));
 
@@ -163,194 +241,240 @@ extern "C" int artea_gpu_index_create_from_hgra(const char* path, const float* v
     if (int rc = dev_alloc(&rs.d_raw, std::max<uint64_t>(rec_words, 1))) return cleanup(rc);
     if (cudaStreamCreateWithFlags(&rs.stream, cudaStreamNonBlocking) != cudaSuccess)
         return cleanup(fail(ARTEA_GPU_ECUDA, "cannot create stream"));
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kReaders; ++i) {
         if (cudaHostAlloc(reinterpret_cast<void**>(&rs.pinned[i]), kChunkWords * 4, cudaHostAllocDefault) !=
                 cudaSuccess ||
             cudaEventCreateWithFlags(&rs.copied[i], cudaEventDisableTiming) != cudaSuccess)
             return cleanup(fail(ARTEA_GPU_ENOMEM, "pinned staging buffers unavailable"));
     }
-    std::vector<uint32_t> hl(n, kNone);
-    std::vector<uint64_t> vrow(n, 0);     // first row of v in file order
-    std::vector<uint32_t> rcnt;           // per row in file order: id count
-    std::vector<uint64_t> rsrc;           // per row in file order: raw word of its first id
-    rcnt.reserve(n);
-    rsrc.reserve(n);
-    uint64_t gsize[64] = {};
-    uint64_t total_ids = 0;
-    uint32_t v = 0;        // vertex whose record is being read
-    int state = 0;         // 0: highest level next, 1: a count next, 2: skipping a row's ids
-    uint32_t lvl = 0;      // level of the next count / the row being skipped
-    uint64_t skip = 0;     // ids of the current row still to skip
-    std::string err;
-    auto row_done = [&]() {
-        if (lvl == 0) {
-            ++v;
-            state = 0;
-        } else {
-            --lvl;
-            state = 1;
-        }
-    };
-    uint64_t chunk = 0;
-    for (uint64_t off = 0; off < rec_words && err.empty(); off += kChunkWords, ++chunk) {
-        const size_t cw = static_cast<size_t>(std::min<uint64_t>(kChunkWords, rec_words - off));
-        const int b = static_cast<int>(chunk & 1);
-        if (cudaEventSynchronize(rs.copied[b]) != cudaSuccess)   // the copy that last read this buffer
-            return cleanup(fail(ARTEA_GPU_ECUDA, "snapshot upload failed"));
-        uint32_t* w = rs.pinned[b];
-        if (std::fread(w, 4, cw, rs.fp) != cw) {
-            err = std::string("short read of ") + path;
-            break;
-        }
-        CUDA_TRY_IX(cudaMemcpyAsync(rs.d_raw + off, w, cw * 4, cudaMemcpyHostToDevice, rs.stream));
-        CUDA_TRY_IX(cudaEventRecord(rs.copied[b], rs.stream));
-        size_t i = 0;
-        while (i < cw) {
-            if (state == 2) {
-                const uint64_t k = std::min<uint64_t>(skip, cw - i);
-                i += k;
-                skip -= k;
-                if (skip == 0) row_done();
-                continue;
+    try {
+        // Per vertex: highest level and first row (file order); per row in file
+        // order: id count and the raw word of its first id. Arrays that every
+        // element of is written before it is read are left uninitialised.
+        std::unique_ptr<uint32_t[]> hl(new uint32_t[n]);
+        std::unique_ptr<uint64_t[]> vrow(new uint64_t[n]);
+        std::vector<uint32_t> rcnt;
+        std::vector<uint64_t> rsrc;
+        const uint64_t row_cap = std::min<uint64_t>(static_cast<uint64_t>(top + 1) * n, rec_words);
+        rcnt.reserve(row_cap);
+        rsrc.reserve(row_cap);
+        uint64_t gsize[kGroupsMax] = {};
+        uint64_t total_ids = 0;
+        uint32_t v = 0;        // vertex whose record is being read
+        int state = 0;         // 0: a record starts, 1: a count next, 2: skipping a row's ids
+        uint32_t lvl = 0;      // level of the next count / the row being skipped
+        uint64_t skip = 0;     // ids of the current row still to skip
+        std::string err;
+        auto row_done = [&]() {
+            if (lvl == 0) {
+                ++v;
+                state = 0;
+            } else {
+                --lvl;
+                state = 1;
             }
-            if (state == 0) {
-                if (v >= n) {
-                    err = "HGRA has trailing bytes";
-                    break;
-                }
-                const uint32_t h = w[i++];
-                hl[v] = h;
-                if (h == kNone) {
+        };
+        const uint64_t nchunks = (rec_words + kChunkWords - 1) / kChunkWords;
+        try {
+            for (int t = 0; t < kReaders && static_cast<uint64_t>(t) < nchunks; ++t)
+                rs.readers.emplace_back(read_chunks, &rs, t, nchunks, rec_words);
+        } catch (...) {
+            rs.stop_readers();
+            return cleanup(fail(ARTEA_GPU_ENOMEM, "cannot start snapshot reader threads"));
+        }
+        for (uint64_t chunk = 0; chunk < nchunks && err.empty(); ++chunk) {
+            const uint64_t off = chunk * kChunkWords;
+            const size_t cw = static_cast<size_t>(std::min<uint64_t>(kChunkWords, rec_words - off));
+            const int b = static_cast<int>(chunk % kReaders);
+            bool read_ok = false;
+            {
+                std::unique_lock<std::mutex> lk(rs.mu);
+                rs.cv.wait(lk, [&] { return rs.holds[b] == chunk; });
+                read_ok = rs.read_ok[b];
+            }
+            if (!read_ok) {
+                err = std::string("short read of ") + path;
+                break;
+            }
+            const uint32_t* w = rs.pinned[b];
+            CUDA_TRY_IX(cudaMemcpyAsync(rs.d_raw + off, w, cw * 4, cudaMemcpyHostToDevice, rs.stream));
+            CUDA_TRY_IX(cudaEventRecord(rs.copied[b], rs.stream));
+            size_t i = 0;
+            while (i < cw) {
+                if (state == 0) {
+                    if (v >= n) {
+                        err = "HGRA has trailing bytes";
+                        break;
+                    }
+                    const uint32_t h = w[i];
+                    if (h == kNone) {
+                        hl[v++] = kNone;
+                        ++i;
+                        continue;
+                    }
+                    if (h > top) {
+                        err = "HGRA vid " + std::to_string(v) + " above top level";
+                        break;
+                    }
+                    hl[v] = h;
+                    gsize[h]++;
+                    vrow[v] = rcnt.size();
+                    // A record that ends inside the chunk is walked row by row;
+                    // one that runs past it continues in the word-by-word states.
+                    size_t p = i + 1;
+                    uint32_t k = 0;
+                    for (; k <= h && p < cw; ++k) p += 1 + static_cast<size_t>(w[p]);
+                    if (k <= h || p > cw) {
+                        lvl = h;
+                        state = 1;
+                        ++i;
+                        continue;
+                    }
+                    p = i + 1;
+                    for (uint32_t l = h;; --l) {
+                        const uint32_t cnt = w[p];
+                        if (cnt > (l == 0 ? bl : ul)) {
+                            err = "HGRA row longer than its level capacity";
+                            break;
+                        }
+                        rcnt.push_back(cnt);
+                        rsrc.push_back(off + p + 1);
+                        total_ids += cnt;
+                        p += 1 + static_cast<size_t>(cnt);
+                        if (l == 0) break;
+                    }
+                    if (!err.empty()) break;
+                    i = p;
                     ++v;
                     continue;
                 }
-                if (h > top) {
-                    err = "HGRA vid " + std::to_string(v) + " above top level";
+                if (state == 2) {
+                    const uint64_t k = std::min<uint64_t>(skip, cw - i);
+                    i += k;
+                    skip -= k;
+                    if (skip == 0) row_done();
+                    continue;
+                }
+                const uint64_t at = off + i;   // raw word of this count
+                const uint32_t cnt = w[i++];
+                const uint32_t capacity = lvl == 0 ? bl : ul;
+                if (cnt > capacity) {
+                    err = "HGRA row longer than its level capacity";
                     break;
                 }
-                gsize[h]++;
-                vrow[v] = rcnt.size();
-                lvl = h;
-                state = 1;
-                continue;
-            }
-            const uint64_t at = off + i;   // raw word of this count
-            const uint32_t cnt = w[i++];
-            const uint32_t capacity = lvl == 0 ? bl : ul;
-            if (cnt > capacity) {
-                err = "HGRA row longer than its level capacity";
-                break;
-            }
-            if (at + 1 + cnt > rec_words) {
-                err = "HGRA truncated in a row";
-                break;
-            }
-            rcnt.push_back(cnt);
-            rsrc.push_back(at + 1);
-            total_ids += cnt;
-            if (cnt == 0) {
-                row_done();
-            } else {
-                skip = cnt;
-                state = 2;
-            }
-        }
-    }
-    if (err.empty() && state == 1) err = "HGRA truncated in vid " + std::to_string(v);
-    if (err.empty() && v < n) err = "HGRA truncated at vid " + std::to_string(v);
-    CUDA_TRY_IX(cudaStreamSynchronize(rs.stream));
-    if (!err.empty()) return cleanup(fail(ARTEA_GPU_EIO, err));
-
-    // ---- vertex table, CSR offsets and the row moves (restore's layout) ----
-    const uint32_t groups = top + 1;
-    std::vector<uint32_t> vinfo(2ull * n);
-    std::vector<uint64_t> gstart(groups + 1, 0);
-    for (uint32_t h = 0; h < groups; ++h) gstart[h + 1] = gstart[h] + gsize[h];
-    std::vector<uint32_t> order(gstart[groups]);   // vertices bucketed by highest level, vid order
-    std::vector<uint64_t> fill(gstart.begin(), gstart.end() - 1);
-    for (uint32_t u = 0; u < n; ++u) {
-        const uint32_t h = hl[u];
-        if (h == kNone) {
-            vinfo[2ull * u] = kNone;
-            vinfo[2ull * u + 1] = kNone;
-            continue;
-        }
-        vinfo[2ull * u] = h;
-        vinfo[2ull * u + 1] = static_cast<uint32_t>(fill[h] - gstart[h]);
-        order[fill[h]++] = u;
-    }
-    uint64_t num_offsets = 0, num_rows = 0;
-    for (uint32_t h = 0; h < groups; ++h) {
-        num_offsets += gsize[h] * (h + 1ull) + 1;
-        num_rows += gsize[h] * (h + 1ull);
-    }
-    std::vector<uint64_t> offs(num_offsets);
-    std::vector<const uint64_t*> gptr(groups);
-    std::vector<unsigned long long> jsrc(num_rows), jdst(num_rows), jlen(num_rows);
-    {
-        uint64_t at = 0, obase = 0, row = 0;
-        for (uint32_t h = 0; h < groups; ++h) {
-            uint64_t* o = offs.data() + obase;
-            gptr[h] = o;
-            uint64_t rr = 0;
-            for (uint64_t k = gstart[h]; k < gstart[h + 1]; ++k) {
-                const uint64_t fr = vrow[order[k]];
-                for (uint32_t j = 0; j <= h; ++j, ++row) {
-                    const uint32_t cnt = rcnt[fr + j];
-                    o[rr++] = at;
-                    jsrc[row] = rsrc[fr + j];
-                    jdst[row] = at;
-                    jlen[row] = cnt | (static_cast<unsigned long long>(h - j) << 32);
-                    at += cnt;
+                if (at + 1 + cnt > rec_words) {
+                    err = "HGRA truncated in a row";
+                    break;
+                }
+                rcnt.push_back(cnt);
+                rsrc.push_back(at + 1);
+                total_ids += cnt;
+                if (cnt == 0) {
+                    row_done();
+                } else {
+                    skip = cnt;
+                    state = 2;
                 }
             }
-            o[rr] = at;
-            obase += gsize[h] * (h + 1ull) + 1;
+            // The buffer goes back to its reader once its copy has completed.
+            CUDA_TRY_IX(cudaEventSynchronize(rs.copied[b]));
+            {
+                std::lock_guard<std::mutex> lk(rs.mu);
+                rs.holds[b] = kFree;
+            }
+            rs.cv.notify_all();
         }
-    }
-    ix->n_offsets = num_offsets;
-    ix->n_nbrs = total_ids;
-    if (int rc = dev_alloc(&ix->d_vinfo, n)) return cleanup(rc);
-    if (int rc = dev_alloc(&ix->d_offsets, num_offsets)) return cleanup(rc);
-    if (int rc = dev_alloc(&ix->d_nbrs, std::max<uint64_t>(total_ids, 1))) return cleanup(rc);
-    if (int rc = dev_alloc(&rs.d_flags, 1)) return cleanup(rc);
-    CUDA_TRY_IX(cudaMemcpy(ix->d_vinfo, vinfo.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice));
-    CUDA_TRY_IX(cudaMemcpy(ix->d_offsets, offs.data(), sizeof(uint64_t) * num_offsets, cudaMemcpyHostToDevice));
-    CUDA_TRY_IX(cudaMemset(rs.d_flags, 0, sizeof(uint32_t)));
-    {
-        uint64_t obase = 0;
+        rs.stop_readers();
+        if (err.empty() && state == 1) err = "HGRA truncated in vid " + std::to_string(v);
+        if (err.empty() && v < n) err = "HGRA truncated at vid " + std::to_string(v);
+        CUDA_TRY_IX(cudaStreamSynchronize(rs.stream));
+        if (!err.empty()) return cleanup(fail(ARTEA_GPU_EIO, err));
+
+        // ---- vertex table and CSR offsets (restore's layout) ----
+        const uint32_t groups = top + 1;
+        std::unique_ptr<uint32_t[]> vinfo(new uint32_t[2ull * n]);
+        uint64_t gstart[kGroupsMax + 1] = {};
+        for (uint32_t h = 0; h < groups; ++h) gstart[h + 1] = gstart[h] + gsize[h];
+        std::unique_ptr<uint32_t[]> order(new uint32_t[gstart[groups]]);   // vertices by highest level, vid order
+        uint64_t fill[kGroupsMax];
+        for (uint32_t h = 0; h < groups; ++h) fill[h] = gstart[h];
+        for (uint32_t u = 0; u < n; ++u) {
+            const uint32_t h = hl[u];
+            if (h == kNone) {
+                vinfo[2ull * u] = kNone;
+                vinfo[2ull * u + 1] = kNone;
+                continue;
+            }
+            vinfo[2ull * u] = h;
+            vinfo[2ull * u + 1] = static_cast<uint32_t>(fill[h] - gstart[h]);
+            order[fill[h]++] = u;
+        }
+        RowGroups gr;
+        std::memset(&gr, 0, sizeof(gr));
+        gr.groups = groups;
+        uint64_t num_offsets = 0;
         for (uint32_t h = 0; h < groups; ++h) {
-            ix->group_ptr[h] = ix->d_offsets + obase;
-            obase += gsize[h] * (h + 1ull) + 1;
+            gr.obase[h] = num_offsets;
+            num_offsets += gsize[h] * (h + 1ull) + 1;
+            gr.row_begin[h + 1] = gr.row_begin[h] + gsize[h] * (h + 1ull);
         }
+        const uint64_t num_rows = gr.row_begin[groups];
+        std::unique_ptr<uint64_t[]> offs(new uint64_t[num_offsets]);
+        std::unique_ptr<unsigned long long[]> csrc(new unsigned long long[std::max<uint64_t>(num_rows, 1)]);
+        std::vector<const uint64_t*> gptr(groups);
+        {
+            uint64_t at = 0, row = 0;
+            for (uint32_t h = 0; h < groups; ++h) {
+                uint64_t* o = offs.get() + gr.obase[h];
+                gptr[h] = o;
+                uint64_t rr = 0;
+                for (uint64_t k = gstart[h]; k < gstart[h + 1]; ++k) {
+                    const uint64_t fr = vrow[order[k]];
+                    for (uint32_t j = 0; j <= h; ++j, ++row) {
+                        o[rr++] = at;
+                        csrc[row] = rsrc[fr + j];
+                        at += rcnt[fr + j];
+                    }
+                }
+                o[rr] = at;
+            }
+        }
+        ix->n_offsets = num_offsets;
+        ix->n_nbrs = total_ids;
+        if (int rc = dev_alloc(&ix->d_vinfo, n)) return cleanup(rc);
+        if (int rc = dev_alloc(&ix->d_offsets, num_offsets)) return cleanup(rc);
+        if (int rc = dev_alloc(&ix->d_nbrs, std::max<uint64_t>(total_ids, 1))) return cleanup(rc);
+        if (int rc = dev_alloc(&rs.d_flags, 1)) return cleanup(rc);
+        CUDA_TRY_IX(cudaMemcpy(ix->d_vinfo, vinfo.get(), sizeof(uint2) * n, cudaMemcpyHostToDevice));
+        CUDA_TRY_IX(cudaMemcpy(ix->d_offsets, offs.get(), sizeof(uint64_t) * num_offsets, cudaMemcpyHostToDevice));
+        CUDA_TRY_IX(cudaMemset(rs.d_flags, 0, sizeof(uint32_t)));
+        for (uint32_t h = 0; h < groups; ++h) ix->group_ptr[h] = ix->d_offsets + gr.obase[h];
+        if (num_rows) {
+            if (int rc = dev_alloc(&rs.d_src, num_rows)) return cleanup(rc);
+            CUDA_TRY_IX(cudaMemcpy(rs.d_src, csrc.get(), sizeof(unsigned long long) * num_rows,
+                                   cudaMemcpyHostToDevice));
+            int sms = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+            const uint64_t want = (num_rows + 7) / 8;   // 8 warps per block
+            const int grid = static_cast<int>(std::min<uint64_t>(want, static_cast<uint64_t>(std::max(sms, 1)) * 16));
+            hgra_rows_kernel<<<grid, 256, 0, rs.stream>>>(rs.d_raw, rs.d_src, gr, ix->d_offsets, ix->d_vinfo, n,
+                                                          ix->d_nbrs, rs.d_flags);
+            CUDA_TRY_IX(cudaGetLastError());
+        }
+        uint32_t flags = 0;
+        CUDA_TRY_IX(cudaMemcpyAsync(&flags, rs.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, rs.stream));
+        CUDA_TRY_IX(cudaStreamSynchronize(rs.stream));
+        dev_free(rs.d_raw);
+        // The reader's check first (EIO), then artea_gpu_graph_validate's (EGRAPH).
+        if (flags & kFlagBadId) return cleanup(fail(ARTEA_GPU_EIO, "HGRA neighbour id out of range"));
+        if (entry >= n) return cleanup(fail(ARTEA_GPU_EGRAPH, "entry point out of range"));
+        if (hl[entry] != top) return cleanup(fail(ARTEA_GPU_EGRAPH, "entry point is not on the top level"));
+        if (flags & kFlagOffLevel)
+            return cleanup(fail(ARTEA_GPU_EGRAPH, "a neighbour id is not on the level of the row that names it"));
+        if (int rc = index_finish_l0(ix, vinfo.get(), gptr.data())) return cleanup(rc);
+    } catch (const std::bad_alloc&) {
+        return cleanup(fail(ARTEA_GPU_ENOMEM, "host memory for the snapshot layout unavailable"));
     }
-    if (num_rows) {
-        if (int rc = dev_alloc(&rs.d_src, num_rows)) return cleanup(rc);
-        if (int rc = dev_alloc(&rs.d_dst, num_rows)) return cleanup(rc);
-        if (int rc = dev_alloc(&rs.d_len, num_rows)) return cleanup(rc);
-        const size_t jb = sizeof(unsigned long long) * num_rows;
-        CUDA_TRY_IX(cudaMemcpy(rs.d_src, jsrc.data(), jb, cudaMemcpyHostToDevice));
-        CUDA_TRY_IX(cudaMemcpy(rs.d_dst, jdst.data(), jb, cudaMemcpyHostToDevice));
-        CUDA_TRY_IX(cudaMemcpy(rs.d_len, jlen.data(), jb, cudaMemcpyHostToDevice));
-        int sms = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        const uint64_t want = (num_rows + 7) / 8;   // 8 warps per block
-        const int grid = static_cast<int>(std::min<uint64_t>(want, static_cast<uint64_t>(std::max(sms, 1)) * 16));
-        hgra_rows_kernel<<<grid, 256, 0, rs.stream>>>(rs.d_raw, rs.d_src, rs.d_dst, rs.d_len, num_rows, ix->d_vinfo,
-                                                      n, ix->d_nbrs, rs.d_flags);
-        CUDA_TRY_IX(cudaGetLastError());
-    }
-    uint32_t flags = 0;
-    CUDA_TRY_IX(cudaMemcpyAsync(&flags, rs.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, rs.stream));
-    CUDA_TRY_IX(cudaStreamSynchronize(rs.stream));
-    dev_free(rs.d_raw);
-    // The reader's check first (EIO), then artea_gpu_graph_validate's (EGRAPH).
-    if (flags & kFlagBadId) return cleanup(fail(ARTEA_GPU_EIO, "HGRA neighbour id out of range"));
-    if (entry >= n) return cleanup(fail(ARTEA_GPU_EGRAPH, "entry point out of range"));
-    if (hl[entry] != top) return cleanup(fail(ARTEA_GPU_EGRAPH, "entry point is not on the top level"));
-    if (flags & kFlagOffLevel)
-        return cleanup(fail(ARTEA_GPU_EGRAPH, "a neighbour id is not on the level of the row that names it"));
-    if (int rc = index_finish_l0(ix, vinfo.data(), gptr.data())) return cleanup(rc);
     *out = ix;
     return ARTEA_GPU_OK;
 }
