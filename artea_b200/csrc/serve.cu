@@ -9,9 +9,10 @@
 // the same search as batch_query on them, so queries of requests that arrive
 // while others are on the GPU overlap on the device. Each warp writes its
 // result row and then a sequence-tagged completion word into mapped host
-// memory, where poll() finds them without any CUDA call. The kernel exits
-// after a bounded idle spin; submit() and poll() relaunch it when published
-// work is pending and it is not running.
+// memory, where poll() finds them without any CUDA call. The kernel stays
+// resident until the server is destroyed; with an idle window set it exits
+// after that long without work, and submit() and poll() relaunch it when
+// published work is pending.
 //
 // There is no serving loop in the reference (its batch_query is one blocking
 // call); the search each query gets is the reference's _query
@@ -178,7 +179,7 @@ struct artea_gpu_server {
     uint64_t consumed_upto = 0;      // every seq below is consumed
     std::vector<uint8_t> consumed;   // per slot, for seq >= consumed_upto
     uint64_t launches = 0;
-    std::mutex mu;
+    mutable std::mutex mu;
 };
 
 namespace {
@@ -428,6 +429,7 @@ extern "C" int artea_gpu_server_poll(artea_gpu_server* s, uint64_t ticket, uint3
 extern "C" int artea_gpu_server_stats(const artea_gpu_server* s, uint64_t* published, uint64_t* consumed,
                                       uint64_t* launches) {
     if (!s || !published || !consumed || !launches) return fail(ARTEA_GPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
     *published = s->next_seq;
     *consumed = s->consumed_upto;
     *launches = s->launches;
