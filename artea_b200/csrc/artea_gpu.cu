@@ -378,8 +378,10 @@ int launch_graph(artea_gpu_router* r, SearchArgs a, bool persistent, const Tunin
     key.nq = p.a.nq;
     key.k_stride = p.a.k_stride;
     key.l0_only = p.a.l0_only;
-    key.tuning = (static_cast<uint64_t>(t.warps) << 32) | (static_cast<uint64_t>(t.stage) << 16) | (t.vh_bits << 1) |
-                 t.regs | (persistent ? 1ull << 63 : 0);
+    // One field per tuning component: warps, staging, table bits, register budget.
+    key.tuning = (static_cast<uint64_t>(t.warps) << 32) | (static_cast<uint64_t>(t.stage) << 24) |
+                 (static_cast<uint64_t>(t.vh_bits) << 8) | static_cast<uint64_t>(t.regs) |
+                 (persistent ? 1ull << 63 : 0);
     auto it = r->graphs.find(key);
     if (it == r->graphs.end()) {
         cudaGraph_t graph = nullptr;
