@@ -158,3 +158,29 @@ def test_serving_percentiles_use_the_reference_profilers_pick():
     assert latency_percentile(list(range(100)), 0.95) == 95.0
     assert latency_percentile([7.0], 0.5) == 7.0
     assert np.isnan(latency_percentile([], 0.5))
+
+
+def test_device_restore_rejects_bad_headers_before_touching_the_gpu(tmp_path):
+    # artea_gpu_index_create_from_hgra checks the header (and the room for one
+    # record per vertex) before it needs a device: the reader's EIO.
+    import struct
+    from artea_b200.router import DeviceIndex
+    base = np.zeros((4, 16), np.float32)
+    good = struct.pack("<7I", 0x48475241, 1, 2, 0, 4, 4, 0) + struct.pack("<6I", 0, 1, 1, 0, 1, 0)
+    cases = {
+        "short": good[:20],
+        "misaligned": good + b"\x00",
+        "magic": b"XXXX" + good[4:],
+        "version": good[:4] + struct.pack("<I", 9) + good[8:],
+        "top_none": good[:12] + struct.pack("<I", 0xFFFFFFFF) + good[16:],
+        "top_64": good[:12] + struct.pack("<I", 64) + good[16:],
+        "entry_range": good[:24] + struct.pack("<I", 5) + good[28:],
+        "no_room": struct.pack("<7I", 0x48475241, 1, 9, 0, 4, 4, 0) + struct.pack("<2I", 0, 0),
+        "empty_trailing": struct.pack("<7I", 0x48475241, 1, 0, 0, 4, 4, 0xFFFFFFFF) + struct.pack("<I", 0),
+    }
+    for name, data in cases.items():
+        p = tmp_path / f"{name}.hgra"
+        p.write_bytes(data)
+        assert _status(lambda: DeviceIndex.from_hgra(str(p), base)) == nat.EIO, name
+        assert _status(lambda: CompactHierarchicalGraph.from_hgra(str(p))) == nat.EIO, name
+    assert _status(lambda: DeviceIndex.from_hgra(str(tmp_path / "missing.hgra"), base)) == nat.EIO
