@@ -493,21 +493,42 @@ int check_kernel_error(artea_gpu_router* r) {
     return ARTEA_GPU_OK;
 }
 
+// host_mapped: queries and/or results are page-locked host memory the kernel
+// reads and writes in place (their transfers overlap the search); such
+// launches read the queries through L2 only and are not captured in graphs,
+// whose keys would then follow the caller's buffers.
 int run_device(artea_gpu_router* r, const float* d_q, uint32_t nq, const uint32_t* d_topk, const uint32_t* d_queue,
-               uint32_t k_stride, uint64_t* d_out, artea_gpu_query_stats* d_stats, bool l0_only, cudaStream_t st) {
+               uint32_t k_stride, uint64_t* d_out, artea_gpu_query_stats* d_stats, bool l0_only, cudaStream_t st,
+               bool host_mapped = false) {
     DeviceGuard guard(r->idx->device);
     if (k_stride == 0 && nq) return fail(ARTEA_GPU_EINVAL, "k_stride must be >= topk");
     if (!d_topk && k_stride < r->topk) return fail(ARTEA_GPU_EINVAL, "k_stride must be >= topk");
     if (nq && (!d_q || !d_out)) return fail(ARTEA_GPU_EINVAL, "null query or output buffer");
+    if (reinterpret_cast<uintptr_t>(d_q) % 16 != 0 || reinterpret_cast<uintptr_t>(d_out) % 8 != 0)
+        return fail(ARTEA_GPU_EINVAL, "queries must be 16-byte and results 8-byte aligned");
     SearchArgs a;
     fill_args(r, &a, d_q, nq, d_topk, d_queue, k_stride, d_out, d_stats, l0_only);
+    if (host_mapped) a.coherent = 1;
     bool persistent = r->schedule != ARTEA_GPU_SCHEDULE_PLAIN;
     Tuning t;
     t.warps = 1;
     t.vh_bits = r->want_vh_bits ? hash_bits_of(r->want_vh_bits) : 0;
     if (persistent) t = tuned(r, a, st);
-    if (r->use_graphs) return launch_graph(r, a, persistent, t, st);
+    if (r->use_graphs && !host_mapped) return launch_graph(r, a, persistent, t, st);
     return launch_with(r, a, persistent, t, st);
+}
+
+// Device address of host memory the GPU reads and writes in place
+// (page-locked and mapped, as all page-locked memory is under unified
+// addressing), or null for pageable memory.
+void* mapped_alias(const void* p) {
+    if (!p) return nullptr;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
 }
 
 }  // namespace
@@ -765,15 +786,27 @@ static int host_query(artea_gpu_router* r, const float* queries, uint32_t nq, co
     DeviceGuard guard(r->idx->device);
     if (int rc = ensure_stage(r, nq, k_stride)) return rc;
     cudaStream_t st = r->stream;
-    CUDA_TRY(cudaMemcpyAsync(r->d_queries, queries, sizeof(float) * static_cast<size_t>(nq) * r->idx->dim,
-                             cudaMemcpyHostToDevice, st));
+    // Page-locked query and result buffers are read and written by the kernel
+    // in place, so their transfers overlap the search; pageable ones are
+    // staged through device buffers.
+    // (The kernel reads query rows as 16-byte vectors and writes 8-byte words.)
+    const float* d_q =
+        reinterpret_cast<uintptr_t>(queries) % 16 == 0 ? static_cast<const float*>(mapped_alias(queries)) : nullptr;
+    uint64_t* d_o = reinterpret_cast<uintptr_t>(out) % 8 == 0 ? static_cast<uint64_t*>(mapped_alias(out)) : nullptr;
+    const bool host_mapped = d_q || d_o;
+    if (!d_q) {
+        CUDA_TRY(cudaMemcpyAsync(r->d_queries, queries, sizeof(float) * static_cast<size_t>(nq) * r->idx->dim,
+                                 cudaMemcpyHostToDevice, st));
+        d_q = r->d_queries;
+    }
     if (topk_pq) CUDA_TRY(cudaMemcpyAsync(r->d_topk, topk_pq, sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
     if (queue_pq) CUDA_TRY(cudaMemcpyAsync(r->d_queue, queue_pq, sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
-    if (int rc = run_device(r, r->d_queries, nq, topk_pq ? r->d_topk : nullptr, queue_pq ? r->d_queue : nullptr,
-                            k_stride, r->d_out, stats ? r->d_stats : nullptr, l0_only, st))
+    if (int rc = run_device(r, d_q, nq, topk_pq ? r->d_topk : nullptr, queue_pq ? r->d_queue : nullptr, k_stride,
+                            d_o ? d_o : r->d_out, stats ? r->d_stats : nullptr, l0_only, st, host_mapped))
         return rc;
-    CUDA_TRY(cudaMemcpyAsync(out, r->d_out, sizeof(uint64_t) * static_cast<size_t>(nq) * k_stride,
-                             cudaMemcpyDeviceToHost, st));
+    if (!d_o)
+        CUDA_TRY(cudaMemcpyAsync(out, r->d_out, sizeof(uint64_t) * static_cast<size_t>(nq) * k_stride,
+                                 cudaMemcpyDeviceToHost, st));
     if (stats)
         CUDA_TRY(cudaMemcpyAsync(stats, r->d_stats, sizeof(artea_gpu_query_stats) * nq, cudaMemcpyDeviceToHost, st));
     return check_kernel_error(r);

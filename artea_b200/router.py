@@ -56,6 +56,17 @@ def metric_code(metric) -> int:
     return int(metric)
 
 
+def _result_buffer(nq: int, k_stride: int) -> np.ndarray:
+    """(nq, k_stride) uint64 result rows in page-locked memory (torch's caching
+    host allocator), which the kernel writes in place: the results reach the
+    host while the search runs instead of in a copy after it."""
+    if nq * k_stride == 0:
+        return np.empty((nq, k_stride), dtype=np.uint64)
+    import torch
+    t = torch.empty(nq * k_stride, dtype=torch.int64, pin_memory=True)
+    return t.numpy().view(np.uint64).reshape(nq, k_stride)
+
+
 class DeviceIndex:
     """A compact graph plus its FP32 vectors, uploaded once to one GPU."""
 
@@ -228,7 +239,7 @@ class GpuRouter:
         qu = None if queue is None else np.ascontiguousarray(queue, dtype=np.uint32)
         if k_stride is None:
             k_stride = int(tk.max()) if tk is not None and tk.size else self.topk
-        out = np.empty((nq, max(k_stride, 0)), dtype=np.uint64)
+        out = _result_buffer(nq, max(k_stride, 0))
         st = (nat.QueryStats * max(nq, 1))() if stats else None
         L = nat.lib()
         if l0_only:

@@ -11,8 +11,10 @@ whose recall@100 reaches 0.95 is timed. One step = one batch_query of all
 
 `value` is device time (CUDA events around each launch on its stream, inputs
 already in HBM, L2 flushed between steps and excluded); `e2e` is the same
-metric through the public C-ABI with host buffers (H2D of queries and D2H of
-results inside the timed region). Multi-GPU runs are replicas (weak scaling):
+metric through the public C-ABI with host buffers inside the timed region: the
+queries sit in page-locked host memory and the router returns its results in
+page-locked memory, so the kernel reads the queries and writes the result rows
+across the bus while it searches (pageable buffers would be staged by copies). Multi-GPU runs are replicas (weak scaling):
 every rank holds the whole index and answers its own batch.
 """
 

@@ -275,3 +275,26 @@ def test_cuda_graph_replay_matches_direct_launches(schedule):
     np.testing.assert_array_equal(g.batch_query(c.queries), c.words[100])
     np.testing.assert_array_equal(g.batch_query(c.queries), c.words[100])
     g.sync()
+
+
+@pytest.mark.parametrize("schedule", ["plain", "persistent"])
+@pytest.mark.parametrize("graphs", [False, True])
+def test_page_locked_host_buffers_are_used_in_place(schedule, graphs):
+    # artea_gpu_batch_query reads page-locked queries and writes page-locked
+    # result rows in place; pageable ones go through device staging. Every mix
+    # returns the reference's words.
+    import torch
+    from artea_b200 import _native as nat
+    c = golden_case("sift2k")
+    nq = c.queries.shape[0]
+    r = GpuRouter(index_for("sift2k"), c.metric, c.topk, 100, mode="exact", schedule=schedule, use_graphs=graphs)
+    qp = torch.from_numpy(np.ascontiguousarray(c.queries)).pin_memory().numpy()
+    for _ in range(2):
+        np.testing.assert_array_equal(r.batch_query(qp), c.words[100])          # both in place
+        np.testing.assert_array_equal(r.batch_query(c.queries), c.words[100])   # staged queries
+        out = np.full((nq, c.topk + 3), 7, np.uint64)                            # staged results, wider rows
+        nat.check(nat.lib().artea_gpu_batch_query(r.handle, nat.ptr(qp), nq, None, None, c.topk + 3, nat.ptr(out),
+                                                  None))
+        np.testing.assert_array_equal(out[:, :c.topk], c.words[100])
+        assert (out[:, c.topk:] == np.uint64((0x7F7FFFFF << 32) | 0x7FFFFFFF)).all()
+    r.close()
