@@ -6,13 +6,14 @@
 // Restore (hierarchical_graph_file_manager.hpp:152-300) buckets vertices by
 // highest level in vid order and lays each group's rows out as one CSR.
 //
-// Here the records stream in fixed chunks through two pinned buffers into a
-// raw copy in device memory. While a chunk is in flight the host walks its
-// record headers only (highest levels and counts; the ids are skipped), which
-// gives the vertex table, the CSR offsets and, for every CSR row, where its
-// ids sit in the raw copy. One kernel then moves every row's ids into place
-// and checks them, so the ids cross the host once (the file read) and are
-// never parsed there. Layout, accepted files and status codes are those of
+// Here reader threads pread the records in fixed chunks into pinned buffers,
+// and each chunk is copied into a raw copy of the records in device memory.
+// While a chunk's copy is in flight the calling thread walks its record
+// headers only (highest levels and counts; the ids are skipped), which gives
+// the vertex table, the CSR offsets and, for every CSR row, where its ids sit
+// in the raw copy. One kernel then moves every row's ids into place and
+// checks them, so the ids cross the host once (the file read) and are never
+// parsed there. Layout, accepted files and status codes are those of
 // artea_gpu_hgra_read followed by artea_gpu_index_create.
 #include <fcntl.h>
 #include <sys/stat.h>
