@@ -92,6 +92,8 @@ def ref_lib():
         L.artea_ref_distance.restype = c_float
         L.artea_ref_distance.argtypes = [c_int, c_void_p, c_void_p, c_uint32]
         L.artea_ref_max_threads.restype = c_int
+        L.artea_ref_restore_layout.restype = c_int
+        L.artea_ref_restore_layout.argtypes = [c_char_p, c_void_p, c_void_p, c_void_p, c_void_p]
         L.artea_ref_restore_seconds.restype = ctypes.c_longlong
         L.artea_ref_restore_seconds.argtypes = [c_char_p, POINTER(c_double)]
         _rlib = L
@@ -112,6 +114,24 @@ def ref_distance(metric: int, a: np.ndarray, b: np.ndarray) -> float:
     a = np.ascontiguousarray(a, dtype=np.float32)
     b = np.ascontiguousarray(b, dtype=np.float32)
     return float(ref_lib().artea_ref_distance(metric, _p(a), _p(b), a.size))
+
+
+def ref_restore_layout(hgra_path: str):
+    """The reference's HierarchicalGraphFileManager::restore of a snapshot as
+    (vertex_info (n, 2) uint32, offsets of all groups concatenated uint64,
+    neighbour ids uint32)."""
+    L = ref_lib()
+    sizes = np.zeros(4, dtype=np.uint64)
+    p = os.fsencode(hgra_path)
+    if L.artea_ref_restore_layout(p, _p(sizes), None, None, None) != 0:
+        raise RuntimeError(L.artea_ref_last_error().decode())
+    n, _, total, ids = (int(x) for x in sizes)
+    vinfo = np.empty((n, 2), dtype=np.uint32)
+    offs = np.empty(max(total, 1), dtype=np.uint64)
+    nbrs = np.empty(max(ids, 1), dtype=np.uint32)
+    if L.artea_ref_restore_layout(p, _p(sizes), _p(vinfo), _p(offs), _p(nbrs)) != 0:
+        raise RuntimeError(L.artea_ref_last_error().decode())
+    return vinfo, offs[:total], nbrs[:ids]
 
 
 def ref_restore_seconds(hgra_path: str) -> float:

@@ -19,6 +19,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <tbb/global_control.h>
@@ -202,6 +203,48 @@ void* artea_ref_open(const char* hgra_path, const float* vecs, uint32_t n, uint3
 }
 
 void artea_ref_close(void* h) { delete static_cast<RefIndex*>(h); }
+
+// The reference's restore of a snapshot in the compact graph's own arrays
+// (index/compact_structure/hierarchical_graph.hpp:46-49, 96-101): sizes[0..3]
+// = vertices, groups, offsets over all groups, neighbour ids; with non-null
+// arrays also vertex_info (highest level, local vid per vertex; invalid
+// levels as 0xFFFFFFFF), the groups' offsets concatenated in level order and
+// the neighbour ids. Returns 0, or -1 on an error.
+int artea_ref_restore_layout(const char* hgra_path, uint64_t* sizes, uint32_t* vertex_info, uint64_t* offsets,
+                             uint32_t* nbrs) {
+    try {
+        auto g = hierarchical_graph_file_manager_t::restore(hgra_path);
+        const uint64_t n = g.get_num_vertices();
+        const auto top = g.top_occupied_level_id();
+        using level_t = std::remove_cv_t<decltype(top)>;
+        const uint64_t groups = n == 0 ? 0 : static_cast<uint64_t>(top) + 1;
+        uint64_t total = 0;
+        for (uint64_t h = 0; h < groups; ++h) total += g.get_nbr_offsets(static_cast<level_t>(h)).size();
+        const auto ids = g.neighbor_ids();
+        sizes[0] = n;
+        sizes[1] = groups;
+        sizes[2] = total;
+        sizes[3] = ids.size();
+        if (!vertex_info) return 0;
+        for (uint64_t v = 0; v < n; ++v) {
+            const auto& info = g.get_vertex_info(static_cast<uint32_t>(v));
+            const bool none = info.highest_level == std::numeric_limits<level_t>::max();
+            vertex_info[2 * v] = none ? 0xFFFFFFFFu : static_cast<uint32_t>(info.highest_level);
+            vertex_info[2 * v + 1] = static_cast<uint32_t>(info.local_vid);
+        }
+        uint64_t at = 0;
+        for (uint64_t h = 0; h < groups; ++h) {
+            const auto off = g.get_nbr_offsets(static_cast<level_t>(h));
+            std::memcpy(offsets + at, off.data(), sizeof(uint64_t) * off.size());
+            at += off.size();
+        }
+        if (!ids.empty()) std::memcpy(nbrs, ids.data(), sizeof(uint32_t) * ids.size());
+        return 0;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
 
 // Seconds taken by hierarchical_graph_file_manager_t::restore of the
 // snapshot alone (index/persistence/hierarchical_graph_file_manager.hpp:152),

@@ -7,7 +7,7 @@ import struct
 import numpy as np
 import pytest
 
-from conftest import golden_case
+from conftest import big_snapshot, golden_case
 from artea_b200 import _native as nat
 from artea_b200.graph import CompactHierarchicalGraph
 from artea_b200.router import DeviceIndex, GpuRouter
@@ -60,54 +60,6 @@ def write_hgra(path, n, top, ul, bl, entry, records):
             words.extend(r)
     with open(path, "wb") as f:
         f.write(struct.pack(f"<{len(words)}I", *words))
-
-
-def big_snapshot(path, n=700_000, seed=7):
-    """~25 M words of vertex records of uneven length (empty rows included),
-    so records cross the 8 M-word staging chunks at every kind of position; a
-    few thousand vertices sit on levels 1 and 2 and 500 are unassigned."""
-    rng = np.random.default_rng(seed)
-    bl, ul = 64, 32
-    hl = np.zeros(n, np.int64)
-    hl[rng.choice(n, 3000, replace=False)] = 1
-    hl[rng.choice(np.nonzero(hl == 1)[0], 40, replace=False)] = 2
-    entry = int(np.nonzero(hl == 2)[0][0])
-    unassigned = np.zeros(n, bool)
-    unassigned[rng.choice(np.nonzero(hl == 0)[0], 500, replace=False)] = True
-    valid0 = np.nonzero(~unassigned)[0].astype(np.uint32)
-    lvl1 = np.nonzero(hl >= 1)[0]
-    lvl2 = np.nonzero(hl == 2)[0]
-    plain = (hl == 0) & ~unassigned
-    cnt0 = rng.integers(0, bl + 1, n)
-    special = {}
-    for v in np.nonzero(hl >= 1)[0]:
-        rec = [int(hl[v])]
-        for lvl in range(int(hl[v]), -1, -1):
-            if lvl == 0:
-                ids = valid0[rng.integers(0, valid0.size, int(cnt0[v]))]
-            else:
-                pool = lvl2 if lvl == 2 else lvl1
-                ids = rng.choice(pool, int(rng.integers(0, min(ul, pool.size) + 1)), replace=False)
-            rec += [len(ids)] + [int(x) for x in ids]
-        special[int(v)] = np.array(rec, np.uint32)
-    rec_len = np.where(unassigned, 1, 2 + cnt0)
-    for v, r in special.items():
-        rec_len[v] = r.size
-    start = 7 + np.concatenate([[0], np.cumsum(rec_len)[:-1]])
-    words = np.zeros(7 + int(rec_len.sum()), np.uint32)
-    words[:7] = [MAGIC, VERSION, n, 2, ul, bl, entry]
-    words[start[unassigned]] = NONE
-    pv = np.nonzero(plain)[0]
-    words[start[pv]] = 0
-    words[start[pv] + 1] = cnt0[pv]
-    c = cnt0[pv]
-    first = np.repeat(start[pv] + 2, c)
-    within = np.arange(int(c.sum())) - np.repeat(np.concatenate([[0], np.cumsum(c)[:-1]]), c)
-    words[first + within] = valid0[rng.integers(0, valid0.size, int(c.sum()))]
-    for v, r in special.items():
-        words[start[v]:start[v] + r.size] = r
-    words.tofile(path)
-    return rng.standard_normal((n, 16)).astype(np.float32)
 
 
 def test_records_straddling_the_staging_chunks(tmp_path):

@@ -224,3 +224,31 @@ def test_oracle_centroid_entry_matches_the_reference_compactor(name, metric):
     bucket = np.nonzero(c.graph.vertex_info[:, 0] == top)[0].astype(np.uint32)
     assert orc.centroid_entry(c.base, metric, bucket) == c.graph.entry_point_vid
     assert orc.centroid_entry(c.base, metric, np.zeros(0, np.uint32)) == 0xFFFFFFFF
+
+
+def _reader_layout(path):
+    from artea_b200.graph import CompactHierarchicalGraph
+    g = CompactHierarchicalGraph.from_hgra(path)
+    offs = np.concatenate(g.group_offsets) if g.num_vertices else np.zeros(0, np.uint64)
+    return g.vertex_info, offs, g.neighbor_ids
+
+
+@pytest.mark.parametrize("name", ["early_stop_top0", "early_stop_top2", "axis80", "sift2k", "deep1k_cos", "gist400"])
+def test_snapshot_reader_layout_is_the_references_restore(name):
+    # hierarchical_graph_file_manager.hpp:152-300: the reference's restore of
+    # the same file gives the same vertex table, group offsets and ids. (The
+    # device restore is held to the host reader word for word on the GPU.)
+    if not orc.have_ref():
+        pytest.skip("reference router not built")
+    for got, want in zip(_reader_layout(golden_case(name).hgra_path), orc.ref_restore_layout(golden_case(name).hgra_path)):
+        np.testing.assert_array_equal(got, want)
+
+
+def test_snapshot_reader_layout_on_a_multi_level_snapshot_with_unassigned_vertices(tmp_path):
+    from conftest import big_snapshot
+    if not orc.have_ref():
+        pytest.skip("reference router not built")
+    path = str(tmp_path / "big.hgra")
+    big_snapshot(path, n=200_000, seed=3)
+    for got, want in zip(_reader_layout(path), orc.ref_restore_layout(path)):
+        np.testing.assert_array_equal(got, want)
