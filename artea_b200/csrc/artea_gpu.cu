@@ -229,8 +229,9 @@ int ensure_stage(artea_gpu_router* r, uint32_t nq, uint32_t k_stride) {
 
 // Persistent grid for a tuning point: as many CTAs per SM as fit.
 int persistent_shape(artea_gpu_router* r, const Tuning& t, LaunchShape* s) {
-    const uint64_t key = (static_cast<uint64_t>(t.warps) << 32) | (static_cast<uint64_t>(t.stage) << 16) |
-                         (t.vh_bits << 1) | t.regs;
+    // One field per tuning component (as in the graph key).
+    const uint64_t key = (static_cast<uint64_t>(t.warps) << 32) | (static_cast<uint64_t>(t.stage) << 24) |
+                         (static_cast<uint64_t>(t.vh_bits) << 8) | static_cast<uint64_t>(t.regs);
     auto hit = r->shapes.find(key);
     if (hit != r->shapes.end()) {
         *s = hit->second;
