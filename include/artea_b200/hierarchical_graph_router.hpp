@@ -13,10 +13,13 @@
 // include/artea_gpu.h. The first batch_query with a graph uploads the graph and
 // base_vecs (the router keeps a const reference to base_vecs, as the reference
 // does, router/vector_router.hpp:46,63-69) and later calls reuse the device
-// copy, keyed by the graph's address. Errors surface as std::runtime_error
+// copy, keyed by the graph's address and checked against a fingerprint of its
+// sizes, storage and a sample of its contents, so a graph restored where a
+// destroyed one lived is uploaded afresh. Errors surface as std::runtime_error
 // (the reference's ARTEA_ERROR, common/logger.hpp:97-99,149).
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -177,6 +180,7 @@ public:
 private:
     struct Device {
         std::mutex mu;   // early-stop setting + launch of one call
+        uint64_t fingerprint = 0;
         artea_gpu_index* index = nullptr;
         artea_gpu_router* router = nullptr;
         ~Device() {
@@ -186,14 +190,54 @@ private:
     };
     struct State {
         std::mutex mu;
-        std::map<const void*, std::unique_ptr<Device>> by_graph;
+        std::map<const void*, std::shared_ptr<Device>> by_graph;
     };
 
+    // Sizes, storage addresses and about 6,000 sampled words of the graph
+    // (splitmix64 steps): a different graph at the same address differs here.
     template <typename HierarchicalGraphT>
-    auto _device_for(const HierarchicalGraphT& g) const -> Device& {
+    static auto _fingerprint(const HierarchicalGraphT& g) -> uint64_t {
+        uint64_t h = 0x9E3779B97F4A7C15ull;
+        auto mix = [&h](uint64_t x) {
+            h ^= x + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+            h ^= h >> 30;
+            h *= 0xBF58476D1CE4E5B9ull;
+            h ^= h >> 27;
+        };
+        const uint32_t n = g.get_num_vertices();
+        const auto top = g.top_occupied_level_id();
+        const auto ids = g.neighbor_ids();
+        mix(n);
+        mix(static_cast<uint64_t>(top));
+        mix(g.entry_point_vid());
+        mix(ids.size());
+        mix(reinterpret_cast<uintptr_t>(ids.data()));
+        for (std::size_t i = 0, step = std::max<std::size_t>(ids.size() / 4096, 1); i < ids.size(); i += step)
+            mix(ids[i]);
+        for (uint32_t v = 0, step = std::max<uint32_t>(n / 1024, 1); v < n; v += step) {
+            const auto& info = g.get_vertex_info(v);
+            mix((static_cast<uint64_t>(info.highest_level) << 32) | info.local_vid);
+        }
+        if (top != HierarchicalGraphT::invalid_level_id) {
+            for (uint32_t lvl = 0; lvl <= static_cast<uint32_t>(top); ++lvl) {
+                const auto off = g.get_nbr_offsets(lvl);
+                mix(reinterpret_cast<uintptr_t>(off.data()));
+                mix(off.size());
+                if (!off.empty()) mix(off.back());
+            }
+        }
+        return h;
+    }
+
+    template <typename HierarchicalGraphT>
+    auto _device_for(const HierarchicalGraphT& g) const -> std::shared_ptr<Device> {
+        const uint64_t fp = _fingerprint(g);
         std::lock_guard<std::mutex> lk(_state->mu);
         auto it = _state->by_graph.find(&g);
-        if (it != _state->by_graph.end()) return *it->second;
+        if (it != _state->by_graph.end()) {
+            if (it->second->fingerprint == fp) return it->second;
+            _state->by_graph.erase(it);   // another graph now lives at this address
+        }
         // compact::HierarchicalGraph -> artea_gpu_graph_desc
         // (compact_structure/hierarchical_graph.hpp:46-49, 83-121).
         const uint32_t n = g.get_num_vertices();
@@ -221,7 +265,8 @@ private:
         d.group_sizes = sizes.data();
         d.neighbor_ids = g.neighbor_ids().data();
         d.num_neighbor_ids = g.neighbor_ids().size();
-        auto dev = std::make_unique<Device>();
+        auto dev = std::make_shared<Device>();
+        dev->fingerprint = fp;
         detail::check(artea_gpu_index_create(&d, _vecs.get_all(), _vecs.get_num_vecs(), _vecs.get_vec_dim(),
                                              _opts.device, &dev->index),
                       "artea_gpu_index_create");
@@ -230,9 +275,8 @@ private:
         o.mode = _opts.mode;
         o.schedule = _opts.schedule;
         detail::check(artea_gpu_router_create(dev->index, _topk, _queue, &o, &dev->router), "artea_gpu_router_create");
-        auto& ref = *dev;
-        _state->by_graph.emplace(&g, std::move(dev));
-        return ref;
+        _state->by_graph.emplace(&g, dev);
+        return dev;
     }
 
     // Per-level configuration thresholds, index = level, for levels 1..top of
@@ -256,7 +300,8 @@ private:
     template <typename HierarchicalGraphT>
     auto _run(const vec_ele_t* queries, uint32_t nq, const HierarchicalGraphT& g, bool l0_only,
               const std::vector<float>& early_stop) const -> knn_results_t {
-        Device& dev = _device_for(g);
+        const std::shared_ptr<Device> held = _device_for(g);   // kept alive for this call
+        Device& dev = *held;
         std::lock_guard<std::mutex> lk(dev.mu);
         const int es = early_stop.empty()
                            ? artea_gpu_router_set_early_stop(dev.router, nullptr, 0)

@@ -10,6 +10,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
+#include <new>
 #include <vector>
 #include <stdexcept>
 #include <string>
@@ -99,8 +101,8 @@ bool early_stop_checks(const Cpu& cpu, const Gpu& gpu, const compact::hierarchic
 }
 
 template <DistanceMetricsT M, vec_dim_t D>
-int run(const compact::hierarchical_graph_t& g, const vector_array_t& base, const vector_array_t& queries,
-        uint32_t topk, uint32_t queue) {
+int run(const char* path, const compact::hierarchical_graph_t& g, const vector_array_t& base,
+        const vector_array_t& queries, uint32_t topk, uint32_t queue) {
     dist_func_t<M, D> dist;
     hierarchical_graph_router_t<M, D> cpu(base, dist, topk, queue);
     cpu.initialize();
@@ -121,18 +123,33 @@ int run(const compact::hierarchical_graph_t& g, const vector_array_t& base, cons
     // back to enable_early_stop=false on the same routers
     ok &= same(cpu.template batch_query<false>(queries, g), gpu.template batch_query<false>(queries, g),
                "batch_query after early stop");
+    // A graph restored where a destroyed one lived is searched as itself, not
+    // as the device copy of its predecessor: an empty graph, then the snapshot
+    // restored into the same storage.
+    {
+        alignas(compact::hierarchical_graph_t) unsigned char slot[sizeof(compact::hierarchical_graph_t)];
+        auto* first = new (slot) compact::hierarchical_graph_t(0, g.ul_max_nbr_size(), g.bl_max_nbr_size(), 0,
+                                                                std::vector<std::size_t>{0});
+        ok &= same(cpu.template batch_query<false>(queries, *first), gpu.template batch_query<false>(queries, *first),
+                   "batch_query on an empty graph");
+        std::destroy_at(first);
+        auto* second = new (slot) compact::hierarchical_graph_t(hierarchical_graph_file_manager_t::restore(path));
+        ok &= same(cpu.template batch_query<false>(queries, *second),
+                   gpu.template batch_query<false>(queries, *second), "batch_query on a graph at a reused address");
+        std::destroy_at(second);
+    }
     std::printf("%s %zu batch entries compared\n", ok ? "OK" : "FAIL", a.size());
     return ok ? 0 : 1;
 }
 
 template <DistanceMetricsT M>
-int by_dim(const compact::hierarchical_graph_t& g, const vector_array_t& base, const vector_array_t& q, uint32_t k,
-           uint32_t L) {
+int by_dim(const char* path, const compact::hierarchical_graph_t& g, const vector_array_t& base,
+           const vector_array_t& q, uint32_t k, uint32_t L) {
     switch (base.get_vec_dim()) {
-        case 16: return run<M, 16>(g, base, q, k, L);
-        case 96: return run<M, 96>(g, base, q, k, L);
-        case 128: return run<M, 128>(g, base, q, k, L);
-        case 960: return run<M, 960>(g, base, q, k, L);
+        case 16: return run<M, 16>(path, g, base, q, k, L);
+        case 96: return run<M, 96>(path, g, base, q, k, L);
+        case 128: return run<M, 128>(path, g, base, q, k, L);
+        case 960: return run<M, 960>(path, g, base, q, k, L);
         default: throw std::runtime_error("unsupported dim");
     }
 }
@@ -169,10 +186,10 @@ int main(int argc, char** argv) {
         const uint32_t k = static_cast<uint32_t>(std::atoi(argv[5]));
         const uint32_t L = static_cast<uint32_t>(std::atoi(argv[6]));
         switch (metric) {
-            case 0: return by_dim<DistanceMetricsT::EUCLIDEAN_SQR>(g, base, queries, k, L);
-            case 1: return by_dim<DistanceMetricsT::EUCLIDEAN>(g, base, queries, k, L);
-            case 2: return by_dim<DistanceMetricsT::COSINE>(g, base, queries, k, L);
-            case 3: return by_dim<DistanceMetricsT::DOT>(g, base, queries, k, L);
+            case 0: return by_dim<DistanceMetricsT::EUCLIDEAN_SQR>(argv[1], g, base, queries, k, L);
+            case 1: return by_dim<DistanceMetricsT::EUCLIDEAN>(argv[1], g, base, queries, k, L);
+            case 2: return by_dim<DistanceMetricsT::COSINE>(argv[1], g, base, queries, k, L);
+            case 3: return by_dim<DistanceMetricsT::DOT>(argv[1], g, base, queries, k, L);
             default: throw std::runtime_error("unknown metric");
         }
     } catch (const std::exception& e) {
