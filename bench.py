@@ -55,6 +55,17 @@ def host_has_avx512() -> bool:
         return False
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def metric_code(name: str) -> int:
     return {"euclidean": 0, "cosine": 2, "dot": 3}[name]
 
@@ -219,7 +230,7 @@ def cpu_baseline(hgra: str, base: np.ndarray, queries: np.ndarray, topk: int, qu
         cores = threads
         kind = "port"
     s = statistics.mean(secs)
-    return {"value": len(q) / s, "unit": "queries/s", "cores": cores, "kind": kind,
+    return {"value": len(q) / s, "unit": "queries/s", "cores": cores, "kind": kind, "cpu_model": cpu_model(),
             "sample": f"{len(q)} queries x {repeats} run(s) of batch_query at queue {queue}, topk {topk}",
             "seconds_per_run": s}
 
@@ -291,7 +302,7 @@ def run_reference_arm(args) -> None:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": {"workload": w.name, "n_base": w.n_base, "n_query": sample,
                                            "dim": w.dim, "metric": w.metric, **cfg},
-            "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample", "cpu_model")},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -413,6 +424,7 @@ def cpu_baseline_uneven(hgra, base, queries, topk, queue, metric, sample):
         info = cpu_baseline(hgra, base, queries[idx], k, L, metric, len(idx))
         total += info["seconds_per_run"]
     return {"value": sample / total, "unit": "queries/s", "cores": info["cores"], "kind": info["kind"],
+            "cpu_model": info["cpu_model"],
             "sample": f"{sample} queries in {len(groups)} (topk, queue) groups, one batch_query per group"}
 
 
@@ -781,7 +793,7 @@ def main() -> None:
                     "h2d_bytes_per_step": int(queries.nbytes), "d2h_bytes_per_step": int(nq * k * 8)},
             "roofline": roofline,
             "cpu_baseline": None if baseline is None else {kk: baseline[kk] for kk in
-                                                           ("value", "unit", "cores", "kind", "sample")},
+                                                           ("value", "unit", "cores", "kind", "sample", "cpu_model")},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "per_query": {"dist_evals": float(st[:, 0].mean()), "l0_rows": float(st[:, 3].mean()),
