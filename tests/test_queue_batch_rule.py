@@ -1,0 +1,142 @@
+"""The batched exact candidate queue of the search kernel against the
+reference's sequential StdCandidateQueue rules, on random tie-heavy inputs.
+
+Reference (router/data_structures/std_candidate_queue.hpp):
+  try_push (:358-388): reject when |T| >= L and d >= lb; else push into the
+    unexplored heap U and the top-L heap T, pop T's maximum by (dist, vid)
+    when |T| > L, and set lb = T.top().dist. Entries evicted from T stay in U.
+  should_terminate (:503-513): U empty -> stop; |T| < L -> go on; else stop
+    when U's minimum has dist > lb.
+  pop_best_unexplored_entry (:398-406): pop U's minimum by (dist, vid).
+
+Kernel (artea_b200/csrc/search.cuh, queue_push_batch / queue_pop_peek): one
+sorted array A of (dist, vid, explored); a row's candidates are accepted at
+once by the closed-form rule
+    accept(j) <=> d_j < lim and #{e in T : e.dist <= d_j} + #{i < j : d_i <= d_j} < L
+(T = A's first min(n, L) entries, lim = lb when A holds L entries), merged
+into A, and A is trimmed to the entries with dist <= lb (ties with lb stay:
+the reference's evicted-but-expandable entries). A pop takes A's first
+unexplored entry; none left is should_terminate.
+
+Both are restated here in Python and run side by side: after every row and
+every pop, T, the set of expandable entries and the popped entry agree.
+"""
+import numpy as np
+import pytest
+
+INF = float("inf")
+
+
+class Sequential:
+    def __init__(self, L):
+        self.L, self.T, self.U, self.lb = L, [], set(), INF
+
+    def push_row(self, row):
+        for d, v in row:
+            if len(self.T) >= self.L and d >= self.lb:
+                continue
+            self.U.add((d, v))
+            self.T.append((d, v))
+            if len(self.T) > self.L:
+                self.T.remove(max(self.T))
+            self.lb = max(self.T)[0]
+
+    def expandable(self):
+        if len(self.T) < self.L:
+            return set(self.U)
+        return {e for e in self.U if e[0] <= self.lb}
+
+    def pop(self):
+        if not self.U or (len(self.T) >= self.L and min(self.U)[0] > self.lb):
+            return None
+        e = min(self.U)
+        self.U.remove(e)
+        return e
+
+
+class Batched:
+    def __init__(self, L):
+        self.L, self.cap, self.A, self.lb = L, 2 * L, [], INF   # A: sorted [d, v, explored]
+
+    def push_row(self, row):
+        L, A = self.L, self.A
+        tn = min(len(A), L)
+        lim = self.lb if len(A) >= L else INF
+        accepted = []
+        for j, (d, v) in enumerate(row):
+            if not d < lim:
+                continue
+            pre = sum(1 for i in range(j) if row[i][0] < lim and row[i][0] <= d)
+            if pre < L and (L - pre - 1 >= tn or A[L - pre - 1][0] > d):
+                accepted.append([d, v, False])
+        if not accepted:
+            return
+        A.extend(accepted)
+        A.sort(key=lambda e: (e[0], e[1]))
+        assert len(A) <= self.cap + len(accepted)
+        del A[self.cap:]
+        if len(A) >= L:
+            self.lb = A[L - 1][0]
+            k = L
+            while k < len(A) and A[k][0] <= self.lb:
+                k += 1
+            del A[k:]
+        assert len(A) <= self.cap, "more than L entries tie lb"
+
+    def top(self):
+        return [(e[0], e[1]) for e in self.A[:min(len(self.A), self.L)]]
+
+    def expandable(self):
+        return {(e[0], e[1]) for e in self.A if not e[2]}
+
+    def pop(self):
+        for e in self.A:
+            if not e[2]:
+                e[2] = True
+                return (e[0], e[1])
+        return None
+
+
+def run_case(rng, L, n_ops, dist_levels, vid_space):
+    seq, bat = Sequential(L), Batched(L)
+    used = set()
+    for _ in range(n_ops):
+        if rng.random() < 0.6:
+            k = int(rng.integers(0, 70))
+            row = []
+            for _ in range(k):
+                v = int(rng.integers(0, vid_space))
+                if v in used:
+                    continue          # the visited set hands each id over once
+                used.add(v)
+                row.append((float(rng.integers(0, dist_levels)), v))
+            seq.push_row(row)
+            bat.push_row(row)
+        else:
+            a, b = seq.pop(), bat.pop()
+            assert a == b, f"pop: sequential {a}, batched {b}"
+        assert sorted(seq.T) == bat.top(), "top-L differs"
+        assert seq.expandable() == bat.expandable(), "expandable entries differ"
+        if len(seq.T) >= L:
+            assert seq.lb == bat.lb
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_batched_queue_equals_sequential_try_push(seed):
+    rng = np.random.default_rng(1000 + seed)
+    for _ in range(500):
+        L = int(rng.integers(1, 12))
+        run_case(rng, L, n_ops=int(rng.integers(5, 40)), dist_levels=int(rng.integers(2, 12)),
+                 vid_space=int(rng.integers(50, 400)))
+
+
+def test_rule_counts_earlier_candidates_of_the_same_row():
+    # A full queue and a row whose later candidates tie earlier accepted ones:
+    # two 1.0 entries fill T (lb = 1.0), so the third 1.0 is rejected
+    # (d >= lb); 0.5 then evicts (1.0, 4), which stays expandable (d == lb).
+    seq, bat = Sequential(2), Batched(2)
+    for q in (seq, bat):
+        q.push_row([(5.0, 1), (6.0, 2)])
+        q.push_row([(1.0, 3), (1.0, 4), (1.0, 5), (0.5, 6)])
+    assert sorted(seq.T) == bat.top() == [(0.5, 6), (1.0, 3)]
+    assert seq.expandable() == bat.expandable()
