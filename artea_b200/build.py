@@ -24,7 +24,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "artea_b200", "csrc")
 LIB_DIR = os.path.join(ROOT, "artea_b200", "lib")
 LIB = os.path.join(LIB_DIR, "libartea_gpu.so")
-REF = os.environ.get("ARTEA_REFERENCE", "/root/reference")
+# The reference checkout: $ARTEA_REFERENCE, else a directory named "reference"
+# beside this repository's root. Without one, the parts compiled from the
+# reference's headers (builder, reference router, drop-in check) are skipped
+# and any copies built earlier are kept.
+REF = os.environ.get("ARTEA_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -65,16 +69,20 @@ def build_cuda(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
-def build_make(subdir: str) -> None:
-    args = ["make", "-C", os.path.join(ROOT, subdir), f"REF={REF}"]
+def build_make(subdir: str, with_ref: bool = True) -> None:
+    args = ["make", "-C", os.path.join(ROOT, subdir)] + ([f"REF={REF}"] if with_ref else [])
     subprocess.run(args, check=True, cwd=ROOT, stdout=subprocess.DEVNULL if not os.environ.get("ARTEA_VERBOSE")
                    else None)
 
 
 def build(force: bool = False) -> None:
     build_cuda(force=force)
-    build_make("oracle")
-    if os.path.isdir(os.path.join(REF, "include")):
+    have_ref = os.path.isdir(os.path.join(REF, "include"))
+    if not have_ref:
+        print(f"[build] no reference checkout at {REF} (set ARTEA_REFERENCE): the reference router, index "
+              "builder and drop-in check are not rebuilt", file=sys.stderr)
+    build_make("oracle", have_ref)
+    if have_ref:
         build_make("index_build")
         build_make(os.path.join("tests", "cpp"))
 
