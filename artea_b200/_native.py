@@ -79,6 +79,9 @@ class RouterOpts(ctypes.Structure):
         ("visited_hash_bits", c_uint32),
         ("register_budget", c_uint32),
         ("stage_rows", c_uint32),
+        ("pipeline", c_uint32),
+        ("prefetch_rows", c_uint32),
+        ("order_queries", c_uint32),
     ]
 
 
@@ -91,6 +94,7 @@ class ServerOpts(ctypes.Structure):
         ("ring_slots", c_uint32),
         ("warps_per_cta", c_uint32),
         ("idle_polls", c_uint32),
+        ("heartbeat_ms", c_uint32),
     ]
 
 
@@ -129,10 +133,12 @@ SIGNATURES = {
     "artea_gpu_server_poll": (c_int, [c_void_p, c_uint64, c_uint32, c_uint32, c_void_p, POINTER(c_int)]),
     "artea_gpu_server_stats": (c_int, [c_void_p, POINTER(c_uint64), POINTER(c_uint64), POINTER(c_uint64)]),
     "artea_gpu_server_destroy": (c_int, [c_void_p]),
+    "artea_gpu_server_pause_heartbeat": (c_int, [c_void_p]),
     "artea_gpu_batch_query_noalloc": (c_int, [c_void_p, c_int, c_int, c_uint32, c_uint32, c_void_p, c_uint32, c_uint32,
                                               c_void_p, c_void_p]),
     "artea_gpu_router_tuning": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32),
                                         POINTER(c_uint32)]),
+    "artea_gpu_router_tuning_ext": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32)]),
 }
 
 

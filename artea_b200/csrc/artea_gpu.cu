@@ -13,6 +13,8 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <sys/stat.h>
+#include <cstdlib>
 
 #include "../../include/artea_gpu.h"
 #include "common.h"
@@ -43,9 +45,17 @@ struct LaunchShape {
 struct Tuning {
     uint32_t warps = 4;
     uint32_t vh_bits = 11;
-    uint32_t regs = 0;   // 0: 85-register budget, 1: 64, 2: 96 (CTAs of at most 4 warps)
+    uint32_t regs = 0;   // 0: 85-register budget, 1: 64, 2: 96, 3: 128 (96 and 128: CTAs of at most 4 warps)
     uint32_t stage = 0;  // 0: rows read with vector loads; kStageRows: TMA-staged in shared memory
+    uint32_t pf = 0;     // pipelined level-0 loop: 1 = the second pass's rows are prefetched into L2
 };
+
+// One field per tuning component (graph keys, the launch-shape cache).
+uint64_t tuning_bits(const Tuning& t) {
+    return (static_cast<uint64_t>(t.warps) << 32) | (static_cast<uint64_t>(t.pf) << 28) |
+           (static_cast<uint64_t>(t.stage) << 24) | (static_cast<uint64_t>(t.vh_bits) << 8) |
+           static_cast<uint64_t>(t.regs);
+}
 
 // Identity of a captured launch: the buffers, sizes and launch parameters.
 struct GraphKey {
@@ -55,6 +65,7 @@ struct GraphKey {
     const void* queue;
     const void* stats;
     const void* phase;
+    const void* order;
     uint32_t nq, k_stride, l0_only, pad;
     uint64_t tuning;
     bool operator<(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) < 0; }
@@ -65,6 +76,7 @@ struct artea_gpu_router {
     uint32_t topk = 0, queue = 0, max_queue = 0, cap = 0, max_batch = 0;
     int metric = 0, mode = 0, schedule = 0;
     uint32_t want_warps = 0, want_ctas_per_sm = 0, want_vh_bits = 0, want_regs = 0, want_stage = 0;
+    uint32_t want_pipeline = 0, want_prefetch = 0, want_order = 0;
     bool use_graphs = false;
     cudaStream_t stream = nullptr;
     int num_sms = 0;
@@ -78,6 +90,7 @@ struct artea_gpu_router {
 
     uint32_t* d_counter = nullptr;
     int* d_error = nullptr;
+    uint32_t* d_order = nullptr;   // query order of the persistent schedule (max_batch entries)
 
     // Staging for host-buffer calls.
     float* d_queries = nullptr;
@@ -89,9 +102,10 @@ struct artea_gpu_router {
 
     uint64_t launches = 0;
     unsigned long long* d_phase = nullptr;      // optional per-query phase cycles (caller-owned)
-    std::map<uint64_t, Tuning> tuned;           // (dim, queue capacity) -> launch parameters
+    std::map<uint64_t, Tuning> tuned;           // (dim, capacity, batch bucket, ...) -> launch parameters
     std::map<uint64_t, LaunchShape> shapes;     // (warps, hash bits) -> persistent grid
     Tuning last;                                // parameters of the last launch
+    bool last_pipe = false, last_ordered = false;
     std::map<GraphKey, cudaGraphExec_t> graphs; // captured launches (use_graphs)
     bool early_stop = false;                    // artea_gpu_router_set_early_stop
     float es_thr[artea_gpu::kMaxGroups] = {};
@@ -127,6 +141,34 @@ __global__ void l0_rows_repeat_kernel(const unsigned long long* __restrict__ l0r
     }
 }
 
+// Query order for the persistent schedule: the batch's query indices sorted by
+// queue size, largest first (counting sort over log2 buckets of the queue
+// size; order within a bucket is arbitrary). Work stealing then starts the
+// longest searches first and the short ones fill the tail. One CTA.
+__global__ void __launch_bounds__(1024) order_by_queue_kernel(const uint32_t* __restrict__ queue, uint32_t nq,
+                                                              uint32_t* __restrict__ order) {
+    __shared__ uint32_t cnt[32];
+    __shared__ uint32_t next[32];
+    if (threadIdx.x < 32) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nq; i += blockDim.x) {
+        const uint32_t L = __ldg(queue + i);
+        atomicAdd(&cnt[L ? 31 - __clz(L) : 0], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        // next[b] = number of queries in the buckets above b (descending order).
+        uint32_t above = 0;
+        for (uint32_t c = threadIdx.x + 1; c < 32; ++c) above += cnt[c];
+        next[threadIdx.x] = above;
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nq; i += blockDim.x) {
+        const uint32_t L = __ldg(queue + i);
+        order[atomicAdd(&next[L ? 31 - __clz(L) : 0], 1u)] = i;
+    }
+}
+
 }  // namespace artea_gpu
 
 namespace {
@@ -149,6 +191,7 @@ KernelFn pick_persistent_s(uint32_t regs) {
     switch (regs) {
         case 1: return search_persistent_kernel<kMetric, kExact, 64, kStage>;
         case 2: return search_persistent_kernel<kMetric, kExact, 96, kStage>;
+        case 3: return kStage ? nullptr : search_persistent_kernel<kMetric, kExact, 128, false>;
         default: return search_persistent_kernel<kMetric, kExact, 85, kStage>;
     }
 }
@@ -158,9 +201,13 @@ KernelFn pick_persistent(uint32_t regs, bool stage) {
     return stage ? pick_persistent_s<kMetric, kExact, true>(regs) : pick_persistent_s<kMetric, kExact, false>(regs);
 }
 
-// Router option register_budget (64, 85, 96) <-> Tuning::regs (1, 0, 2).
-uint32_t regs_index(uint32_t budget) { return budget == 64 ? 1u : (budget == 96 ? 2u : 0u); }
-uint32_t regs_budget(uint32_t index) { return index == 1 ? 64u : (index == 2 ? 96u : 85u); }
+// Router option register_budget (64, 85, 96, 128) <-> Tuning::regs (1, 0, 2, 3).
+uint32_t regs_index(uint32_t budget) {
+    return budget == 64 ? 1u : (budget == 96 ? 2u : (budget == 128 ? 3u : 0u));
+}
+uint32_t regs_budget(uint32_t index) {
+    return index == 1 ? 64u : (index == 2 ? 96u : (index == 3 ? 128u : 85u));
+}
 
 template <int kMetric>
 KernelFn pick_kernel_m(bool exact, bool persistent, uint32_t regs, bool stage) {
@@ -229,17 +276,16 @@ int ensure_stage(artea_gpu_router* r, uint32_t nq, uint32_t k_stride) {
 
 // Persistent grid for a tuning point: as many CTAs per SM as fit.
 int persistent_shape(artea_gpu_router* r, const Tuning& t, LaunchShape* s) {
-    // One field per tuning component (as in the graph key).
-    const uint64_t key = (static_cast<uint64_t>(t.warps) << 32) | (static_cast<uint64_t>(t.stage) << 24) |
-                         (static_cast<uint64_t>(t.vh_bits) << 8) | static_cast<uint64_t>(t.regs);
+    const uint64_t key = tuning_bits(t);
     auto hit = r->shapes.find(key);
     if (hit != r->shapes.end()) {
         *s = hit->second;
         return ARTEA_GPU_OK;
     }
-    if (t.regs == 2 && t.warps > 4)
-        return fail(ARTEA_GPU_EINVAL, "register budget 96 allows at most 4 warps per CTA");
+    if ((t.regs == 2 || t.regs == 3) && t.warps > 4)
+        return fail(ARTEA_GPU_EINVAL, "register budgets 96 and 128 allow at most 4 warps per CTA");
     KernelFn fn = pick_kernel(r->metric, r->mode == ARTEA_GPU_MODE_EXACT, true, t.regs, t.stage != 0);
+    if (!fn) return fail(ARTEA_GPU_EINVAL, "no kernel for this combination (staged rows with the 128-register budget)");
     const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits, t.stage) * t.warps;
     if (smem > 227u * 1024u) return fail(ARTEA_GPU_EINVAL, "persistent CTA needs more than 227 KB shared memory");
     CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -291,6 +337,8 @@ int fill_args(artea_gpu_router* r, SearchArgs* a, const float* d_q, uint32_t nq,
     a->phase_cycles = r->d_phase;
     a->early_stop = r->early_stop ? 1u : 0u;
     for (int h = 0; h < kMaxGroups; ++h) a->es_thr[h] = r->es_thr[h];
+    // The pipelined level-0 loop takes whole rows of distinct ids, <= 64 each.
+    a->l0_pipe = (r->want_pipeline != kNoHash && ix->l0_unique && ix->bl <= 64u) ? 1u : 0u;
     return ARTEA_GPU_OK;
 }
 
@@ -303,13 +351,14 @@ struct Prepared {
     uint32_t threads = 0;
     uint32_t smem = 0;
     bool persistent = false;
+    bool order = false;       // run order_by_queue_kernel first (a.order is set)
     SearchArgs a;
 };
 
 int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning& t, Prepared* p) {
     const bool exact = r->mode == ARTEA_GPU_MODE_EXACT;
     KernelFn fn = pick_kernel(r->metric, exact, persistent, t.regs, persistent && t.stage != 0);
-    if (!fn) return fail(ARTEA_GPU_EINVAL, "unknown metric");
+    if (!fn) return fail(ARTEA_GPU_EINVAL, "no kernel for this metric and option combination");
     a.vh_bits = t.vh_bits;
     {
         uint32_t kb = 1;
@@ -337,6 +386,16 @@ int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tun
     }
     a.vis_bits = r->d_vis_bits;
     a.vis_list = r->d_vis_list;
+    a.pf_l2 = t.pf;
+    // Longest searches first: only with per-query queue sizes (else every
+    // query has the same size) and on the persistent schedule.
+    p->order = persistent && a.queue != nullptr && a.nq > 1 && r->want_order != kNoHash;
+    if (p->order) {
+        if (!r->d_order) {
+            if (int rc = dev_alloc(&r->d_order, r->max_batch)) return rc;
+        }
+        a.order = r->d_order;
+    }
     // The attribute is per kernel function and other launch shapes (other
     // routers, autotuner candidates) change it: set it for every launch.
     CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -347,6 +406,10 @@ int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tun
 
 int enqueue(artea_gpu_router* r, const Prepared& p, cudaStream_t st) {
     if (p.persistent) CUDA_TRY(cudaMemsetAsync(r->d_counter, 0, sizeof(uint32_t), st));
+    if (p.order) {
+        order_by_queue_kernel<<<1, 1024, 0, st>>>(p.a.queue, p.a.nq, r->d_order);
+        CUDA_TRY(cudaGetLastError());
+    }
     p.fn<<<p.grid, p.threads, p.smem, st>>>(p.a);
     CUDA_TRY(cudaGetLastError());
     return ARTEA_GPU_OK;
@@ -358,6 +421,8 @@ int launch_with(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning
     if (int rc = prepare_launch(r, a, persistent, t, &p)) return rc;
     if (int rc = enqueue(r, p, st)) return rc;
     r->last = t;
+    r->last_pipe = p.a.l0_pipe != 0;
+    r->last_ordered = p.order;
     r->launches++;
     return ARTEA_GPU_OK;
 }
@@ -379,10 +444,8 @@ int launch_graph(artea_gpu_router* r, SearchArgs a, bool persistent, const Tunin
     key.nq = p.a.nq;
     key.k_stride = p.a.k_stride;
     key.l0_only = p.a.l0_only;
-    // One field per tuning component: warps, staging, table bits, register budget.
-    key.tuning = (static_cast<uint64_t>(t.warps) << 32) | (static_cast<uint64_t>(t.stage) << 24) |
-                 (static_cast<uint64_t>(t.vh_bits) << 8) | static_cast<uint64_t>(t.regs) |
-                 (persistent ? 1ull << 63 : 0);
+    key.order = p.a.order;
+    key.tuning = tuning_bits(t) | (persistent ? 1ull << 63 : 0) | (p.a.l0_pipe ? 1ull << 62 : 0);
     auto it = r->graphs.find(key);
     if (it == r->graphs.end()) {
         cudaGraph_t graph = nullptr;
@@ -402,80 +465,206 @@ int launch_graph(artea_gpu_router* r, SearchArgs a, bool persistent, const Tunin
     }
     CUDA_TRY(cudaGraphLaunch(it->second, st));
     r->last = t;
+    r->last_pipe = p.a.l0_pipe != 0;
+    r->last_ordered = p.order;
     r->launches++;
     return ARTEA_GPU_OK;
 }
 
-// Autotuner: warps per CTA and visited-hash size for the persistent schedule,
-// picked per (dim, queue capacity) by timing each candidate on the first
-// call's batch (one warm and one timed launch each).
+// Autotuner for the persistent schedule. The first call for a (dim, queue
+// capacity, batch-size bucket, per-query arrays) combination times each
+// candidate on that call's batch (one warm launch, then the median of three
+// timed launches, on the call's stream, waiting for each) and keeps the
+// fastest: warps per CTA x visited-table size x register budget first; then,
+// at the best of those, rows loaded ahead (8 or 16) and TMA-staged rows (at
+// the best table size). Picks are kept per router and, for routers that fix
+// none of these options, in a text file (ARTEA_TUNING_CACHE; default
+// $XDG_CACHE_HOME/artea_b200/tuning.txt, else ~/.cache/artea_b200/tuning.txt;
+// an empty ARTEA_TUNING_CACHE turns the file off) keyed by the GPU model, SM
+// count, this library's build, the metric, mode, graph size and the
+// combination above, so later processes skip the timing.
+const char* kBuildId = __DATE__ " " __TIME__;
+
+std::string tuning_cache_path() {
+    const char* env = std::getenv("ARTEA_TUNING_CACHE");
+    if (env) return std::string(env);
+    const char* xdg = std::getenv("XDG_CACHE_HOME");
+    if (xdg && *xdg) return std::string(xdg) + "/artea_b200/tuning.txt";
+    const char* home = std::getenv("HOME");
+    if (home && *home) return std::string(home) + "/.cache/artea_b200/tuning.txt";
+    return std::string();
+}
+
+std::mutex g_tuning_file_mu;
+
+std::string tuning_file_key(const artea_gpu_router* r, uint64_t key) {
+    cudaDeviceProp prop;
+    std::string gpu = "gpu";
+    if (cudaGetDeviceProperties(&prop, r->idx->device) == cudaSuccess) gpu = prop.name;
+    else cudaGetLastError();
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "%s|%d|%s|m%d|x%d|n%u|k%llx|cs%u|p%u|o%u", gpu.c_str(), r->num_sms, kBuildId,
+                  r->metric, r->mode, r->idx->n, static_cast<unsigned long long>(key), r->want_ctas_per_sm,
+                  r->want_pipeline, r->want_order);
+    std::string k(buf);
+    for (char& c : k)
+        if (c == ' ') c = '_';
+    return k;
+}
+
+bool tuning_file_load(const std::string& path, const std::string& fkey, Tuning* t) {
+    if (path.empty()) return false;
+    std::lock_guard<std::mutex> lk(g_tuning_file_mu);
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return false;
+    char line[1024];
+    bool found = false;
+    while (std::fgets(line, sizeof(line), f)) {
+        char k[600];
+        unsigned w, b, rg, st, pf;
+        if (std::sscanf(line, "%599s %u %u %u %u %u", k, &w, &b, &rg, &st, &pf) == 6 && fkey == k && rg <= 3 &&
+            (st == 0 || st == kStageRows) && pf <= 1 && w >= 1 && w <= 8 && b <= 12) {
+            t->warps = w;
+            t->vh_bits = b;
+            t->regs = rg;
+            t->stage = st;
+            t->pf = pf;
+            found = true;   // the last line for a key wins
+        }
+    }
+    std::fclose(f);
+    return found;
+}
+
+void tuning_file_store(const std::string& path, const std::string& fkey, const Tuning& t) {
+    if (path.empty()) return;
+    std::lock_guard<std::mutex> lk(g_tuning_file_mu);
+    const size_t slash = path.find_last_of('/');
+    if (slash != std::string::npos && slash > 0) {
+        const std::string dir = path.substr(0, slash);   // mkdir -p, one component at a time
+        for (size_t i = 1; i <= dir.size(); ++i)
+            if (i == dir.size() || dir[i] == '/') mkdir(dir.substr(0, i).c_str(), 0755);
+    }
+    FILE* f = std::fopen(path.c_str(), "a");
+    if (!f) return;
+    std::fprintf(f, "%s %u %u %u %u %u\n", fkey.c_str(), t.warps, t.vh_bits, t.regs, t.stage, t.pf);
+    std::fclose(f);
+}
+
+uint32_t batch_bucket(uint32_t nq) {
+    uint32_t b = 0;
+    while (b < 31 && (1u << b) < nq) ++b;
+    return b;
+}
+
 Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     Tuning t;
-    if (r->want_warps && r->want_vh_bits && r->want_regs && r->want_stage) {
+    const bool fixed_pf = r->want_prefetch != 0 || !a.l0_pipe;
+    const uint32_t pf_fixed = r->want_prefetch == 16 ? 1u : 0u;
+    if (r->want_warps && r->want_vh_bits && r->want_regs && r->want_stage && fixed_pf) {
         t.warps = r->want_warps;
         t.vh_bits = hash_bits_of(r->want_vh_bits);
         t.regs = regs_index(r->want_regs);
         t.stage = stage_of(r->want_stage);
+        t.pf = pf_fixed;
         return t;
     }
-    const uint64_t key = (static_cast<uint64_t>(r->idx->dim) << 32) | r->cap;
+    const uint64_t key = (static_cast<uint64_t>(r->idx->dim) << 40) | (static_cast<uint64_t>(r->cap) << 16) |
+                         (static_cast<uint64_t>(batch_bucket(a.nq)) << 8) | (a.queue ? 2u : 0u) |
+                         (a.l0_only ? 1u : 0u);
     auto it = r->tuned.find(key);
     if (it != r->tuned.end()) return it->second;
+    const bool shared = !r->want_warps && !r->want_vh_bits && !r->want_regs && !r->want_stage && !r->want_prefetch;
+    const std::string path = shared ? tuning_cache_path() : std::string();
+    const std::string fkey = shared ? tuning_file_key(r, key) : std::string();
+    if (shared && tuning_file_load(path, fkey, &t)) {
+        r->tuned[key] = t;
+        return t;
+    }
     // Candidate lists: a fixed option is its own single choice.
-    std::vector<uint32_t> warp_choices = {2, 4, 8}, bit_choices = {0, 8, 9, 10}, reg_choices = {0, 1, 2},
-                          stage_choices = {0, kStageRows};
+    std::vector<uint32_t> warp_choices = {2, 4, 8}, bit_choices = {0, 8, 9, 10}, reg_choices = {0, 1, 2, 3},
+                          stage_choices = {0, kStageRows}, pf_choices = {0, 1};
     if (r->want_warps) warp_choices = {r->want_warps};
     if (r->want_vh_bits) bit_choices = {hash_bits_of(r->want_vh_bits)};
     if (r->want_regs) reg_choices = {regs_index(r->want_regs)};
     if (r->want_stage) stage_choices = {stage_of(r->want_stage)};
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    if (fixed_pf) pf_choices = {pf_fixed};
+    cudaEvent_t ev[4];
+    for (auto& e : ev) cudaEventCreate(&e);
     float best_ms = 1e30f;
     Tuning best;
     best.warps = warp_choices[0];
     best.vh_bits = bit_choices[0];
     best.regs = reg_choices[0];
     best.stage = stage_choices[0];
-    // Row staging is timed at every register budget and warp count but only
-    // with the best table size found without it.
-    for (uint32_t stage : stage_choices)
-    for (uint32_t reg : reg_choices)
-    for (uint32_t w : warp_choices) {
-        for (uint32_t b : bit_choices) {
-            if (stage && stage_choices.size() > 1 && bit_choices.size() > 1 && b != best.vh_bits) continue;
-            Tuning c;
-            c.warps = w;
-            c.vh_bits = b;
-            c.regs = reg;
-            c.stage = stage;
-            LaunchShape s;
-            if (persistent_shape(r, c, &s) != ARTEA_GPU_OK) {
-                cudaGetLastError();
-                continue;
-            }
-            float ms = 0.f;
-            bool ok = true;
-            for (int rep = 0; rep < 2 && ok; ++rep) {
-                cudaEventRecord(e0, st);
-                ok = launch_with(r, a, true, c, st) == ARTEA_GPU_OK;
-                cudaEventRecord(e1, st);
-                ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
-            }
-            if (!ok) {
-                cudaGetLastError();
-                continue;
-            }
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best_ms) {
-                best_ms = ms;
-                best = c;
-            }
+    best.pf = pf_choices[0];
+    auto time_candidate = [&](const Tuning& c) {
+        if (c.stage && c.pf) return;           // staged rows use the one-expansion loop
+        if (c.stage && c.regs == 3) return;    // no staged 128-register kernel
+        if ((c.regs == 2 || c.regs == 3) && c.warps > 4) return;
+        LaunchShape s;
+        if (persistent_shape(r, c, &s) != ARTEA_GPU_OK) {
+            cudaGetLastError();
+            return;
         }
+        // One warm launch, then the median of three.
+        bool ok = launch_with(r, a, true, c, st) == ARTEA_GPU_OK;
+        for (int rep = 0; rep < 3 && ok; ++rep) {
+            cudaEventRecord(ev[rep], st);
+            ok = launch_with(r, a, true, c, st) == ARTEA_GPU_OK;
+        }
+        if (ok) cudaEventRecord(ev[3], st);
+        ok = ok && cudaEventSynchronize(ev[3]) == cudaSuccess;
+        if (!ok) {
+            cudaGetLastError();
+            return;
+        }
+        float ms[3];
+        cudaEventElapsedTime(&ms[0], ev[0], ev[1]);
+        cudaEventElapsedTime(&ms[1], ev[1], ev[2]);
+        cudaEventElapsedTime(&ms[2], ev[2], ev[3]);
+        std::sort(ms, ms + 3);
+        if (ms[1] < best_ms) {
+            best_ms = ms[1];
+            best = c;
+        }
+    };
+    // 1. launch shape, table size and register budget, with vector loads.
+    for (uint32_t reg : reg_choices)
+        for (uint32_t w : warp_choices)
+            for (uint32_t b : bit_choices) {
+                Tuning c;
+                c.warps = w;
+                c.vh_bits = b;
+                c.regs = reg;
+                c.stage = stage_choices[0];
+                c.pf = pf_choices[0];
+                time_candidate(c);
+            }
+    // 2. rows loaded ahead, at the best shape.
+    for (size_t i = 1; i < pf_choices.size(); ++i) {
+        Tuning c = best;
+        c.pf = pf_choices[i];
+        time_candidate(c);
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    // 3. TMA-staged rows at every register budget and warp count, with the
+    // best table size found so far.
+    for (size_t i = 1; i < stage_choices.size(); ++i) {
+        const uint32_t bits = best.vh_bits;
+        for (uint32_t reg : reg_choices)
+            for (uint32_t w : warp_choices) {
+                Tuning c;
+                c.warps = w;
+                c.vh_bits = bits;
+                c.regs = reg;
+                c.stage = stage_choices[i];
+                c.pf = 0;
+                time_candidate(c);
+            }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
     r->tuned[key] = best;
+    if (shared && best_ms < 1e29f) tuning_file_store(path, fkey, best);
     return best;
 }
 
@@ -514,6 +703,7 @@ int run_device(artea_gpu_router* r, const float* d_q, uint32_t nq, const uint32_
     Tuning t;
     t.warps = 1;
     t.vh_bits = r->want_vh_bits ? hash_bits_of(r->want_vh_bits) : 0;
+    t.pf = r->want_prefetch == 16 ? 1u : 0u;
     if (persistent) t = tuned(r, a, st);
     if (r->use_graphs && !host_mapped) return launch_graph(r, a, persistent, t, st);
     return launch_with(r, a, persistent, t, st);
@@ -703,13 +893,20 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
     if (o.mode != ARTEA_GPU_MODE_EXACT && o.mode != ARTEA_GPU_MODE_FAST) return fail(ARTEA_GPU_EINVAL, "unknown mode");
     if (o.schedule < 0 || o.schedule > 2) return fail(ARTEA_GPU_EINVAL, "unknown schedule");
     if (o.warps_per_cta > 8) return fail(ARTEA_GPU_EINVAL, "warps_per_cta must be <= 8");
-    if (o.register_budget != 0 && o.register_budget != 64 && o.register_budget != 85 && o.register_budget != 96)
-        return fail(ARTEA_GPU_EINVAL, "register_budget must be 0 (autotuned), 64, 85 or 96");
+    if (o.register_budget != 0 && o.register_budget != 64 && o.register_budget != 85 && o.register_budget != 96 &&
+        o.register_budget != 128)
+        return fail(ARTEA_GPU_EINVAL, "register_budget must be 0 (autotuned), 64, 85, 96 or 128");
     if (o.visited_hash_bits != 0 && o.visited_hash_bits != 0xffffffffu &&
         (o.visited_hash_bits < 6 || o.visited_hash_bits > 12))
         return fail(ARTEA_GPU_EINVAL, "visited_hash_bits must be 0 (autotuned), ~0 (no table) or in [6, 12]");
     if (o.stage_rows != 0 && o.stage_rows != 0xffffffffu && o.stage_rows != kStageRows)
         return fail(ARTEA_GPU_EINVAL, "stage_rows must be 0 (autotuned), ~0 (vector loads) or 8");
+    if (o.pipeline != 0 && o.pipeline != 1 && o.pipeline != 0xffffffffu)
+        return fail(ARTEA_GPU_EINVAL, "pipeline must be 0 (where the graph allows), 1 or ~0 (off)");
+    if (o.prefetch_rows != 0 && o.prefetch_rows != 8 && o.prefetch_rows != 16)
+        return fail(ARTEA_GPU_EINVAL, "prefetch_rows must be 0 (autotuned), 8 or 16");
+    if (o.order_queries != 0 && o.order_queries != 0xffffffffu)
+        return fail(ARTEA_GPU_EINVAL, "order_queries must be 0 (largest queue first) or ~0 (index order)");
     DeviceGuard guard(ix->device);
     auto* r = new artea_gpu_router();
     r->idx = ix;
@@ -726,6 +923,9 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
     r->want_vh_bits = o.visited_hash_bits;
     r->want_regs = o.register_budget;
     r->want_stage = o.stage_rows;
+    r->want_pipeline = o.pipeline;
+    r->want_prefetch = o.prefetch_rows;
+    r->want_order = o.order_queries;
     r->use_graphs = o.use_graphs != 0;
     r->words_per_slot = ((static_cast<uint64_t>(ix->n) + 127) / 128) * 4;   // multiple of 4 words
     r->list_cap = std::max<uint32_t>(std::min<uint32_t>(ix->n, 32768), 64);
@@ -755,6 +955,7 @@ int artea_gpu_router_destroy(artea_gpu_router* r) {
     dev_free(r->d_vis_list);
     dev_free(r->d_counter);
     dev_free(r->d_error);
+    dev_free(r->d_order);
     dev_free(r->d_queries);
     dev_free(r->d_out);
     dev_free(r->d_topk);
@@ -880,6 +1081,15 @@ int artea_gpu_router_tuning(const artea_gpu_router* r, uint32_t* warps_per_cta, 
     *visited_hash_bits = r->last.vh_bits;
     *register_budget = regs_budget(r->last.regs);
     *stage_rows = r->last.stage;
+    return ARTEA_GPU_OK;
+}
+
+int artea_gpu_router_tuning_ext(const artea_gpu_router* r, uint32_t* pipeline, uint32_t* prefetch_rows,
+                                uint32_t* ordered) {
+    if (!r || !pipeline || !prefetch_rows || !ordered) return fail(ARTEA_GPU_EINVAL, "null argument");
+    *pipeline = r->last_pipe ? 1u : 0u;
+    *prefetch_rows = r->last.pf ? 16u : 8u;
+    *ordered = r->last_ordered ? 1u : 0u;
     return ARTEA_GPU_OK;
 }
 

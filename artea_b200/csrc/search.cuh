@@ -89,6 +89,9 @@ struct SearchArgs {
     uint32_t coherent;        // queries/topk/queue may change while the kernel runs (serving ring)
     uint32_t early_stop;      // stop level-h greedy walks at distance <= es_thr[h]
     float es_thr[kMaxGroups]; // per-level thresholds in query distance units
+    uint32_t l0_pipe;         // level-0 rows hold <= 64 distinct ids: pipelined level-0 loop
+    uint32_t pf_l2;           // pipelined loop: also prefetch the second pass's rows into L2
+    const uint32_t* __restrict__ order;   // persistent schedule: query order (null: 0..nq-1)
 };
 
 // Phase-cycle breakdown written per query when phase_cycles is set.
@@ -245,10 +248,52 @@ struct Stage {
     uint32_t phase;      // parity of the next phase to wait for
 };
 
-// Distances for cnt candidates (ids in cvid, shared memory) into cdist.
-template <int kMetric, bool kExact, bool kStage>
+// Loads of the next expansion's rows, issued ahead of its distance phase so
+// they are in flight while the warp merges the current batch. With kRegs, the
+// first pass's first block of chunks (rows cvid[0, 8), one float4 per chunk
+// and lane) is loaded into x, which batch_distances then consumes (kPre);
+// without, those rows' first 512 bytes are prefetched into L2 (one 128-byte
+// line per lane). With l2_next, the second pass's rows (cvid[8, 16)) are
+// prefetched into L2 as well.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+template <bool kRegs>
+__device__ __forceinline__ void dist_preload(const DeviceGraph& g, const uint32_t* cvid, uint32_t cnt,
+                                             ulonglong2 (&x)[kBlock], bool l2_next) {
+    const int lane = lane_id();
+    const uint32_t r = static_cast<uint32_t>(lane) >> 2;
+    const uint32_t gi = lane & 3;
+    const uint32_t dim = g.dim;
+    const uint32_t off = 128u * gi;   // byte offset of this lane's line in a row
+    if (kRegs) {
+        const uint32_t nchunks = dim >> 4;
+        const bool valid = r < cnt;
+        const uint32_t vid = valid ? cvid[r] : 0u;
+        const float* row = g.vecs + static_cast<size_t>(vid) * dim + 4 * gi;
+#pragma unroll
+        for (int k = 0; k < kBlock; ++k) {
+            const ulonglong2* src = reinterpret_cast<const ulonglong2*>(row + 16 * k);
+            x[k] = (valid && static_cast<uint32_t>(k) < nchunks) ? __ldg(src) : make_ulonglong2(0ull, 0ull);
+        }
+    } else if (r < cnt && off < dim * 4u) {
+        prefetch_l2(reinterpret_cast<const char*>(g.vecs + static_cast<size_t>(cvid[r]) * dim) + off);
+    }
+    if (l2_next && cnt > 8u) {
+        const uint32_t r2 = 8u + r;
+        if (r2 < cnt && off < dim * 4u)
+            prefetch_l2(reinterpret_cast<const char*>(g.vecs + static_cast<size_t>(cvid[r2]) * dim) + off);
+    }
+}
+
+// Distances for cnt candidates (ids in cvid, shared memory) into cdist. With
+// kPre, the first pass's first block of chunks is taken from pre (loaded by
+// dist_preload<true> on the same cvid) instead of being loaded here.
+template <int kMetric, bool kExact, bool kStage, bool kPre = false>
 __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ q, float qsq,
-                                const uint32_t* cvid, float* cdist, uint32_t cnt, Stage& st, int* error) {
+                                const uint32_t* cvid, float* cdist, uint32_t cnt, Stage& st, int* error,
+                                const ulonglong2 (*pre)[kBlock] = nullptr) {
     const int lane = lane_id();
     const int r = lane >> 2;
     const int gi = lane & 3;
@@ -285,10 +330,15 @@ __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ 
         f32x2 B01 = 0ull, B23 = 0ull;   // cos: x*x
         for (uint32_t cb = 0; cb < nchunks; cb += kBlock) {
             ulonglong2 x[kBlock];
+            if (kPre && p == 0 && cb == 0) {
 #pragma unroll
-            for (int k = 0; k < kBlock; ++k) {
-                const ulonglong2* src = reinterpret_cast<const ulonglong2*>(row + 16 * (cb + k));
-                x[k] = (valid && cb + k < nchunks) ? (kStage ? *src : __ldg(src)) : make_ulonglong2(0ull, 0ull);
+                for (int k = 0; k < kBlock; ++k) x[k] = (*pre)[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < kBlock; ++k) {
+                    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(row + 16 * (cb + k));
+                    x[k] = (valid && cb + k < nchunks) ? (kStage ? *src : __ldg(src)) : make_ulonglong2(0ull, 0ull);
+                }
             }
 #pragma unroll
             for (int k = 0; k < kBlock; ++k) {
@@ -722,7 +772,9 @@ __device__ __forceinline__ int queue_pop_peek(Queue& q, int* next) {
     return first;
 }
 
-// try_push for a whole batch at once (std_candidate_queue.hpp:358-388).
+// try_push for a whole batch at once (std_candidate_queue.hpp:358-388), in
+// two steps: queue_accept decides which candidates the sequential pushes
+// would accept, queue_merge applies them.
 // Sequentially, candidate j is rejected iff T already holds L entries at
 // distance <= d_j. A rejected candidate never enters T, and every later
 // candidate at a distance >= a rejected one is rejected too, so candidate j
@@ -732,10 +784,11 @@ __device__ __forceinline__ int queue_pop_peek(Queue& q, int* next) {
 // merged into the sorted array in one pass; trimming the result at the new
 // lb yields exactly the state the sequential pushes leave (entries trimmed
 // in between are worse than every later lb).
-// Scratch: bd/bv hold the accepted batch; cdist/cvid are reused for its
-// sorted copy.
-__device__ inline void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, uint32_t cnt, float* bd, uint32_t* bv,
-                                 int* error) {
+//
+// queue_accept writes the accepted candidates (m <= cnt <= kCandBatch), in
+// candidate order, to bd/bv and returns m.
+__device__ inline uint32_t queue_accept(const Queue& q, const uint32_t* cvid, const float* cdist, uint32_t cnt,
+                                        float* bd, uint32_t* bv) {
     const int lane = lane_id();
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t tn = min(q.n, q.L);
@@ -798,22 +851,47 @@ __device__ inline void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, 
         improving_before += __popc(imask);
     }
     __syncwarp();
+    return m;
+}
+
+// Merges the m (<= kCandBatch) accepted entries of bd/bv into the sorted
+// array and trims it at the new lb. The batch is first sorted by (dist, vid)
+// in place (each lane holds at most two entries in registers). A vid word may
+// carry the explored bit (an entry popped before it is merged); ordering
+// ignores it.
+__device__ inline void queue_merge(Queue& q, float* bd, uint32_t* bv, uint32_t m) {
+    const int lane = lane_id();
     if (m == 0) return;
-    // Sort the accepted batch by (dist, vid) into cdist/cvid (ranks are unique).
-    for (uint32_t k = lane; k < m; k += 32) {
-        const float d = bd[k];
-        const uint32_t v = bv[k];
-        uint32_t r = 0;
-        for (uint32_t i = 0; i < m; ++i) r += entry_less(bd[i], bv[i], d, v) ? 1u : 0u;
-        cdist[r] = d;
-        cvid[r] = v;
+    {
+        float sd[2];
+        uint32_t sv[2], rk[2];
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            const uint32_t k = lane + 32u * t;
+            rk[t] = 0xffffffffu;
+            if (k < m) {
+                sd[t] = bd[k];
+                sv[t] = bv[k];
+                uint32_t r = 0;
+                for (uint32_t i = 0; i < m; ++i) r += entry_less(bd[i], bv[i], sd[t], sv[t]) ? 1u : 0u;
+                rk[t] = r;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            if (rk[t] != 0xffffffffu) {
+                bd[rk[t]] = sd[t];
+                bv[rk[t]] = sv[t];
+            }
+        }
+        __syncwarp();
     }
-    __syncwarp();
     // Final positions of the batch entries: rank in the old array + rank in the batch.
     uint32_t posb[2] = {0xffffffffu, 0xffffffffu};
     for (uint32_t r = lane, t = 0; r < m; r += 32, ++t) {
-        const float d = cdist[r];
-        const uint32_t v = cvid[r];
+        const float d = bd[r];
+        const uint32_t v = bv[r];
         uint32_t lo = 0, hi = q.n;
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
@@ -837,7 +915,7 @@ __device__ inline void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, 
             uint32_t lo = 0, hi = m;
             while (lo < hi) {
                 const uint32_t mid = (lo + hi) >> 1;
-                if (entry_less(cdist[mid], cvid[mid], dd, vv)) lo = mid + 1; else hi = mid;
+                if (entry_less(bd[mid], bv[mid], dd, vv)) lo = mid + 1; else hi = mid;
             }
             np = static_cast<uint32_t>(i) + lo;
         }
@@ -846,7 +924,7 @@ __device__ inline void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, 
         __syncwarp();
     }
     for (uint32_t r = lane, t = 0; r < m; r += 32, ++t) {
-        if (posb[t] < q.cap) { q.d[posb[t]] = cdist[r]; q.v[posb[t]] = cvid[r] & kVidMask; }
+        if (posb[t] < q.cap) { q.d[posb[t]] = bd[r]; q.v[posb[t]] = bv[r]; }
     }
     __syncwarp();
     const uint32_t total = min(q.n + m, q.cap);
@@ -863,7 +941,36 @@ __device__ inline void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, 
         }
         q.n = newn;
     }
+}
+
+// try_push of a whole batch (bd/bv: scratch for the accepted entries).
+__device__ inline void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, uint32_t cnt, float* bd, uint32_t* bv,
+                                        int* error) {
+    queue_merge(q, bd, bv, queue_accept(q, cvid, cdist, cnt, bd, bv));
     (void)error;
+}
+
+// The smallest accepted entry of bd/bv[0, m) by (dist, vid), m >= 1: its index
+// (in every lane), distance and vid word.
+__device__ __forceinline__ uint32_t batch_argmin(const float* bd, const uint32_t* bv, uint32_t m, float* d_out,
+                                                 uint32_t* v_out) {
+    const int lane = lane_id();
+    float md = INFINITY;
+    uint32_t mv = 0xffffffffu, mi = 0xffffffffu;
+    for (uint32_t k = lane; k < m; k += 32) {
+        const float d = bd[k];
+        const uint32_t v = bv[k];
+        if (mi == 0xffffffffu || entry_less(d, v, md, mv)) { md = d; mv = v; mi = k; }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        const float od = __shfl_xor_sync(kFull, md, off);
+        const uint32_t ov = __shfl_xor_sync(kFull, mv, off);
+        const uint32_t oi = __shfl_xor_sync(kFull, mi, off);
+        if (oi != 0xffffffffu && (mi == 0xffffffffu || entry_less(od, ov, md, mv))) { md = od; mv = ov; mi = oi; }
+    }
+    *d_out = md;
+    *v_out = mv;
+    return mi;
 }
 
 // ---------------------------------------------------------------------------
@@ -961,12 +1068,146 @@ __device__ __forceinline__ WarpSmem carve(float* base, uint32_t dim, uint32_t ca
 }
 
 // ---------------------------------------------------------------------------
+// Level-0 beam search, pipelined across expansions (single_layer_router.hpp:
+// 145-163, beam_loop.hpp:90-119), for graphs whose level-0 rows hold at most 64
+// distinct ids. On entry the queue holds the cursor and the cursor is visited.
+//
+// The reference pops the next entry only after pushing every candidate of the
+// current row. That entry is known earlier: once the current batch's
+// acceptance is decided, the next pop is the smaller (by dist, vid) of
+//   * p2, the first unexplored entry after the one being expanded, and
+//   * the smallest accepted candidate of the batch,
+// because every other unexplored entry is larger than p2, rejected candidates
+// never enter the unexplored heap, and the smallest accepted candidate always
+// ends inside the top L (all entries before it are old entries, fewer than L
+// by its acceptance). p2 cannot be trimmed by the merge either: if it is the
+// smaller, it is at most the smallest accepted candidate, which stays within
+// lb. With neither, should_terminate holds (std_candidate_queue.hpp:503-513).
+// So the next expansion's row is collected (visited test_and_set; the merge
+// does not touch the visited set) and its first rows' loads are issued before
+// the current batch is merged, and the merge runs while they are in flight.
+// The chosen entry is marked explored where it lies: p2 in the array, a new
+// candidate in the batch before the merge places it.
+// ---------------------------------------------------------------------------
+template <int kMetric, bool kExact, bool kRegs>
+__device__ __forceinline__ void l0_search_pipelined(const SearchArgs& a, Queue& q, Visited& vs, const WarpSmem& sm,
+                                                    float qsq, uint32_t cur, Counters& ct, PhaseClock& pc,
+                                                    Stage& st) {
+    const int lane = lane_id();
+    const DeviceGraph& g = a.g;
+    const bool l2_next = a.pf_l2 != 0;
+    uint32_t* cv = sm.cvid;
+    float* cd = sm.cdist;
+    // Pop the cursor: the queue's only entry.
+    if (lane == 0) q.v[0] |= kExplored;
+    __syncwarp();
+    q.hint = 1;
+    unsigned long long desc = __ldg(g.l0row + cur);
+    uint32_t len = static_cast<uint32_t>(desc >> kRowLenShift);
+    const uint32_t* row = g.nbrs + (desc & kRowStartMask);
+    uint32_t ids0 = lane < len ? __ldg(row + lane) : 0xffffffffu;
+    uint32_t ids1 = lane + 32 < len ? __ldg(row + lane + 32) : 0xffffffffu;
+    uint32_t cnt = collect_row64_unique(g, vs, ids0, ids1, len, cv, a.error);
+    ct.l0_rows++;
+    ct.l0_row_ids += len;
+    ulonglong2 pre[kBlock];
+    dist_preload<kRegs>(g, cv, cnt, pre, l2_next);
+    pc.lap(kPhCollect);
+    // The predicted entry after the one being expanded: its index (-1: none),
+    // vid, row descriptor and, once loaded, ids.
+    int p2 = -1;
+    uint32_t pf_vid = kVidMask;
+    unsigned long long pf_desc = 0ull;
+    uint32_t pf_ids0 = 0u, pf_ids1 = 0u;
+    bool pf_have_ids = false;
+    for (uint32_t it = 0;; ++it) {
+        if (it > g.n) { set_error(a.error, kErrBound); break; }
+        if (cnt) batch_distances<kMetric, kExact, false, kRegs>(g, sm.q, qsq, cv, cd, cnt, st, a.error, &pre);
+        ct.dist_evals += cnt;
+        if (p2 >= 0 && !pf_have_ids) {
+            // The predicted entry's descriptor has arrived by now: fetch its ids.
+            const uint32_t len2 = static_cast<uint32_t>(pf_desc >> kRowLenShift);
+            const uint32_t* row2 = g.nbrs + (pf_desc & kRowStartMask);
+            pf_ids0 = lane < len2 ? __ldg(row2 + lane) : 0xffffffffu;
+            pf_ids1 = lane + 32 < len2 ? __ldg(row2 + lane + 32) : 0xffffffffu;
+            pf_have_ids = true;
+        }
+        pc.lap(kPhDist);
+        const uint32_t m = cnt ? queue_accept(q, cv, cd, cnt, sm.bd, sm.bv) : 0u;
+        // The next pop: min(p2, smallest accepted), or termination.
+        bool take_new = false;
+        uint32_t next = kVidMask;
+        if (m) {
+            float bdm;
+            uint32_t bvm;
+            const uint32_t bi = batch_argmin(sm.bd, sm.bv, m, &bdm, &bvm);
+            take_new = p2 < 0 || entry_less(bdm, bvm, q.d[p2], q.v[p2]);
+            if (take_new) {
+                next = bvm & kVidMask;
+                if (lane == 0) sm.bv[bi] = bvm | kExplored;
+            }
+        }
+        if (!take_new && p2 >= 0) {
+            next = q.v[p2] & kVidMask;
+            if (lane == 0) q.v[p2] |= kExplored;
+            q.hint = static_cast<uint32_t>(p2) + 1;
+        }
+        __syncwarp();
+        // CandidateEntry::is_invalid ends the loop as the reference's pop of an
+        // invalid entry does (cannot occur on validated graphs).
+        const bool go = (take_new || p2 >= 0) && next != kVidMask;
+        uint32_t ncnt = 0;
+        if (go) {
+            const bool hit = !take_new && next == pf_vid;
+            if (hit) pc.count(kPhPrefetchHits);
+            desc = hit ? pf_desc : __ldg(g.l0row + next);
+            len = static_cast<uint32_t>(desc >> kRowLenShift);
+            row = g.nbrs + (desc & kRowStartMask);
+            if (hit && pf_have_ids) {
+                ids0 = pf_ids0;
+                ids1 = pf_ids1;
+            } else {
+                ids0 = lane < len ? __ldg(row + lane) : 0xffffffffu;
+                ids1 = lane + 32 < len ? __ldg(row + lane + 32) : 0xffffffffu;
+            }
+            pf_have_ids = false;
+            pc.lap(kPhPop);
+            // The current candidates are in bd/bv now: cv takes the next row's.
+            ncnt = collect_row64_unique(g, vs, ids0, ids1, len, cv, a.error);
+            ct.l0_rows++;
+            ct.l0_row_ids += len;
+            dist_preload<kRegs>(g, cv, ncnt, pre, l2_next);
+            pc.lap(kPhCollect);
+        }
+        // The current batch's merge runs while the next rows are loaded.
+        queue_merge(q, sm.bd, sm.bv, m);
+        __syncwarp();
+        pc.lap(kPhMerge);
+        if (!go) break;
+        // Predict the entry after `next`: the first unexplored entry now.
+        p2 = queue_find_unexplored(q, q.hint);
+        if (p2 >= 0) {
+            q.hint = static_cast<uint32_t>(p2);
+            pf_vid = q.v[p2] & kVidMask;
+            pf_desc = __ldg(g.l0row + pf_vid);
+        } else {
+            q.hint = q.n;
+            pf_vid = kVidMask;
+        }
+        pc.lap(kPhPop);
+        cnt = ncnt;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // One query (hierarchical_graph_router.hpp:195-248; query_l0_only :258-286).
 // ---------------------------------------------------------------------------
 // stage_phase: with kStage, the parity of the next phase of the warp's staging
 // mbarrier, which the caller initialised once (an mbarrier is not initialised
 // again while it is valid) and which carries over from query to query.
-template <int kMetric, bool kExact, bool kStage = false>
+// kRegs: the pipelined level-0 loop holds the next expansion's first pass in
+// registers (the 128-register budget) instead of prefetching it into L2.
+template <int kMetric, bool kExact, bool kStage = false, bool kRegs = false>
 __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, const WarpSmem& sm,
                            uint32_t* stage_phase = nullptr) {
     const int lane = lane_id();
@@ -1086,71 +1327,75 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
         q.lb = FLT_MAX;
         queue_insert(q, cur_d, cur, a.error);
         visited_set(vs, cur);
-        // Software pipeline: while one row is processed, the row descriptor and
-        // then the neighbour ids of the entry that would be expanded next are
-        // already being loaded (used if that entry is indeed popped next).
-        uint32_t pf_vid = cur;
-        unsigned long long pf_desc = __ldg(g.l0row + cur);
-        uint32_t pf_ids0 = 0u, pf_ids1 = 0u;
-        bool pf_have_ids = false;
-        for (uint32_t it = 0;; ++it) {
-            if (it > g.n) { set_error(a.error, kErrBound); break; }
-            int p2;
-            const int p = queue_pop_peek(q, &p2);
-            if (p < 0) break;
-            const uint32_t v = q.v[p] & kVidMask;
-            if (v == kVidMask) break;   // CandidateEntry::is_invalid
-            const bool hit = v == pf_vid;
-            if (hit) pc.count(kPhPrefetchHits);
-            const unsigned long long desc = hit ? pf_desc : __ldg(g.l0row + v);
-            const uint32_t len = static_cast<uint32_t>(desc >> kRowLenShift);
-            const uint32_t* row = g.nbrs + (desc & kRowStartMask);
-            uint32_t ids0, ids1;
-            if (hit && pf_have_ids) {
-                ids0 = pf_ids0;
-                ids1 = pf_ids1;
-            } else {
-                ids0 = lane < len ? __ldg(row + lane) : 0xffffffffu;
-                ids1 = lane + 32 < len ? __ldg(row + lane + 32) : 0xffffffffu;
-            }
-            pf_have_ids = false;
-            if (p2 >= 0) {
-                pf_vid = q.v[p2] & kVidMask;
-                pf_desc = __ldg(g.l0row + pf_vid);
-            } else {
-                pf_vid = kVidMask;
-            }
-            ct.l0_rows++;
-            ct.l0_row_ids += len;
-            pc.lap(kPhPop);
-            uint32_t pos = 0;
-            const bool one_pass = g.l0_unique && len <= 64u;
-            while (pos < len) {
-                uint32_t cnt, consumed;
-                if (one_pass) {
-                    cnt = collect_row64_unique(g, vs, ids0, ids1, len, cvid, a.error);
-                    consumed = len;
+        if (!kStage && a.l0_pipe) {
+            l0_search_pipelined<kMetric, kExact, kRegs>(a, q, vs, sm, qsq, cur, ct, pc, st);
+        } else {
+            // Software pipeline: while one row is processed, the row descriptor and
+            // then the neighbour ids of the entry that would be expanded next are
+            // already being loaded (used if that entry is indeed popped next).
+            uint32_t pf_vid = cur;
+            unsigned long long pf_desc = __ldg(g.l0row + cur);
+            uint32_t pf_ids0 = 0u, pf_ids1 = 0u;
+            bool pf_have_ids = false;
+            for (uint32_t it = 0;; ++it) {
+                if (it > g.n) { set_error(a.error, kErrBound); break; }
+                int p2;
+                const int p = queue_pop_peek(q, &p2);
+                if (p < 0) break;
+                const uint32_t v = q.v[p] & kVidMask;
+                if (v == kVidMask) break;   // CandidateEntry::is_invalid
+                const bool hit = v == pf_vid;
+                if (hit) pc.count(kPhPrefetchHits);
+                const unsigned long long desc = hit ? pf_desc : __ldg(g.l0row + v);
+                const uint32_t len = static_cast<uint32_t>(desc >> kRowLenShift);
+                const uint32_t* row = g.nbrs + (desc & kRowStartMask);
+                uint32_t ids0, ids1;
+                if (hit && pf_have_ids) {
+                    ids0 = pf_ids0;
+                    ids1 = pf_ids1;
                 } else {
-                    collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error, ids0, ids1, pos == 0);
+                    ids0 = lane < len ? __ldg(row + lane) : 0xffffffffu;
+                    ids1 = lane + 32 < len ? __ldg(row + lane + 32) : 0xffffffffu;
                 }
-                pos = consumed;
-                pc.lap(kPhCollect);
-                if (cnt == 0) continue;
-                batch_distances<kMetric, kExact, kStage>(g, sm.q, qsq, cvid, cdist, cnt, st, a.error);
-                ct.dist_evals += cnt;
-                pc.lap(kPhDist);
-                if (p2 >= 0 && !pf_have_ids) {
-                    // The next entry's descriptor has arrived by now: fetch its ids
-                    // while the merge runs.
-                    const uint32_t len2 = static_cast<uint32_t>(pf_desc >> kRowLenShift);
-                    const uint32_t* row2 = g.nbrs + (pf_desc & kRowStartMask);
-                    pf_ids0 = lane < len2 ? __ldg(row2 + lane) : 0xffffffffu;
-                    pf_ids1 = lane + 32 < len2 ? __ldg(row2 + lane + 32) : 0xffffffffu;
-                    pf_have_ids = true;
+                pf_have_ids = false;
+                if (p2 >= 0) {
+                    pf_vid = q.v[p2] & kVidMask;
+                    pf_desc = __ldg(g.l0row + pf_vid);
+                } else {
+                    pf_vid = kVidMask;
                 }
-                queue_push_batch(q, cvid, cdist, cnt, sm.bd, sm.bv, a.error);
-                __syncwarp();
-                pc.lap(kPhMerge);
+                ct.l0_rows++;
+                ct.l0_row_ids += len;
+                pc.lap(kPhPop);
+                uint32_t pos = 0;
+                const bool one_pass = g.l0_unique && len <= 64u;
+                while (pos < len) {
+                    uint32_t cnt, consumed;
+                    if (one_pass) {
+                        cnt = collect_row64_unique(g, vs, ids0, ids1, len, cvid, a.error);
+                        consumed = len;
+                    } else {
+                        collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error, ids0, ids1, pos == 0);
+                    }
+                    pos = consumed;
+                    pc.lap(kPhCollect);
+                    if (cnt == 0) continue;
+                    batch_distances<kMetric, kExact, kStage>(g, sm.q, qsq, cvid, cdist, cnt, st, a.error);
+                    ct.dist_evals += cnt;
+                    pc.lap(kPhDist);
+                    if (p2 >= 0 && !pf_have_ids) {
+                        // The next entry's descriptor has arrived by now: fetch its ids
+                        // while the merge runs.
+                        const uint32_t len2 = static_cast<uint32_t>(pf_desc >> kRowLenShift);
+                        const uint32_t* row2 = g.nbrs + (pf_desc & kRowStartMask);
+                        pf_ids0 = lane < len2 ? __ldg(row2 + lane) : 0xffffffffu;
+                        pf_ids1 = lane + 32 < len2 ? __ldg(row2 + lane + 32) : 0xffffffffu;
+                        pf_have_ids = true;
+                    }
+                    queue_push_batch(q, cvid, cdist, cnt, sm.bd, sm.bv, a.error);
+                    __syncwarp();
+                    pc.lap(kPhMerge);
+                }
             }
         }
         visited_clear(vs);
@@ -1202,13 +1447,17 @@ __global__ void __launch_bounds__(32, 24) search_plain_kernel(SearchArgs a) {
     search_one<kMetric, kExact>(a, qi, qi, sm);
 }
 
-// Persistent schedule: warps pull query indices from a shared counter.
-// kBudget sets the register budget through the launch bounds: 64 (4 CTAs of
-// 256 threads per SM, 32 resident warps), 85 (3 x 256: 80 registers used, 24
-// warps) or 96 (5 CTAs of at most 128 threads: 20 warps, the search state
-// without spills). (__maxnreg__ with the same counts measured slower.)
-constexpr int budget_threads(int budget) { return budget == 96 ? 128 : 256; }
-constexpr int budget_min_blocks(int budget) { return budget == 64 ? 4 : (budget == 96 ? 5 : 3); }
+// Persistent schedule: warps pull query indices from a shared counter (in
+// the order a.order gives, if set). kBudget sets the register budget through
+// the launch bounds: 64 (4 CTAs of 256 threads per SM, 32 resident warps), 85
+// (3 x 256: 80 registers used, 24 warps), 96 (5 CTAs of at most 128 threads:
+// 20 warps) or 128 (4 CTAs of at most 128 threads: 16 warps; the pipelined
+// level-0 loop then holds the next expansion's first rows in registers).
+// (__maxnreg__ with the same counts measured slower.)
+constexpr int budget_threads(int budget) { return budget >= 96 ? 128 : 256; }
+constexpr int budget_min_blocks(int budget) {
+    return budget == 64 ? 4 : (budget == 96 ? 5 : (budget == 128 ? 4 : 3));
+}
 
 template <int kMetric, bool kExact, int kBudget, bool kStage = false>
 __global__ void __launch_bounds__(budget_threads(kBudget), budget_min_blocks(kBudget))
@@ -1230,7 +1479,8 @@ __global__ void __launch_bounds__(budget_threads(kBudget), budget_min_blocks(kBu
         if (lane_id() == 0) qi = atomicAdd(a.next_query, 1u);
         qi = __shfl_sync(kFull, qi, 0);
         if (qi >= a.nq) break;
-        search_one<kMetric, kExact, kStage>(a, qi, slot, sm, &stage_phase);
+        if (a.order) qi = __ldg(a.order + qi);
+        search_one<kMetric, kExact, kStage, kBudget == 128>(a, qi, slot, sm, &stage_phase);
     }
     if (kStage) {
         __syncwarp();

@@ -10,18 +10,24 @@
 // while others are on the GPU overlap on the device. Each warp writes its
 // result row and then a sequence-tagged completion word into mapped host
 // memory, where poll() finds them without any CUDA call. The kernel stays
-// resident until the server is destroyed; with an idle window set it exits
-// after that long without work, and submit() and poll() relaunch it when
-// published work is pending.
+// resident until the server is destroyed, or until the library's heartbeat
+// (a counter in mapped host memory that a host thread of the server advances
+// every few milliseconds) has not moved for heartbeat_ms: an idle warp that
+// sees that closes the ring and the kernel ends, so no wait of the kernel
+// outlives its host by more than that; submit() and poll() then return
+// ARTEA_GPU_ETIMEOUT.
 //
 // There is no serving loop in the reference (its batch_query is one blocking
 // call); the search each query gets is the reference's _query
 // (router/hierarchical_graph_router.hpp:195-248), bit for bit in EXACT mode.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -35,10 +41,15 @@ struct ServeCtl {
     const volatile uint32_t* tail;    // sequences published so far (device, written by host copies)
     const volatile uint32_t* stop;    // set by the host to end the kernel
     volatile uint32_t* done;          // mapped host memory: done[slot] = seq + 1 when finished
-    volatile uint32_t* closed;        // mapped host memory: set to 1 by the warp that closes the ring
+    volatile uint32_t* closed;        // mapped host memory: kClosedIdle / kClosedHeartbeat by the closing warp
+    const volatile uint32_t* beat;    // mapped host memory: the host's heartbeat counter
     uint32_t ring;                    // ring slots; slot = seq % ring
-    uint32_t idle_limit;              // microseconds without work before the kernel exits
+    uint32_t idle_limit;              // microseconds without work before the kernel exits (~0: never)
+    uint32_t beat_limit_ms;           // the kernel ends once the heartbeat has not moved for this long
 };
+
+constexpr uint32_t kClosedIdle = 1u;        // an idle window ended the instance
+constexpr uint32_t kClosedHeartbeat = 2u;   // the host's heartbeat went stale
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -65,6 +76,9 @@ __global__ void __launch_bounds__(256, 3) serve_kernel(SearchArgs a, ServeCtl c)
     const volatile unsigned long long* vhead = c.head;
     unsigned long long idle_since = 0;
     uint32_t backoff = 64;
+    uint32_t beat_seen = *c.beat;
+    unsigned long long beat_since = global_ns();
+    unsigned long long beat_checked = beat_since;
     for (;;) {
         uint32_t seq = 0;
         int state = 0;   // 0: nothing claimed, 1: claimed seq, 2: ring closed
@@ -91,16 +105,25 @@ __global__ void __launch_bounds__(256, 3) serve_kernel(SearchArgs a, ServeCtl c)
         if (state == 0) {
             const unsigned long long now = global_ns();
             if (idle_since == 0) idle_since = now;
-            if (now - idle_since > 1000ull * c.idle_limit) {
+            if (now - beat_checked > 10000000ull) {   // read host memory at most every 10 ms
+                beat_checked = now;
+                const uint32_t beat = *c.beat;
+                if (beat != beat_seen) {
+                    beat_seen = beat;
+                    beat_since = now;
+                }
+            }
+            const bool stale = now - beat_since > 1000000ull * c.beat_limit_ms;
+            if (stale || (c.idle_limit != 0xFFFFFFFFu && now - idle_since > 1000ull * c.idle_limit)) {
                 if (lane == 0) {
                     const unsigned long long cur = *vhead;
                     const uint32_t t = *c.tail;
-                    if (!(cur >> 32) && static_cast<int32_t>(t - static_cast<uint32_t>(cur)) <= 0 &&
+                    // A stale heartbeat closes the ring whatever it holds: the
+                    // host that would collect the results no longer answers.
+                    if (!(cur >> 32) && (stale || static_cast<int32_t>(t - static_cast<uint32_t>(cur)) <= 0) &&
                         atomicCAS(c.head, cur, cur | (1ull << 32)) == cur) {
-                        // Tell the host this instance is ending (it relaunches
-                        // on the same stream, after this instance, when work
-                        // is pending).
-                        *c.closed = 1u;
+                        // Tell the host why this instance is ending.
+                        *c.closed = stale ? kClosedHeartbeat : kClosedIdle;
                         __threadfence_system();
                     }
                 }
@@ -155,8 +178,16 @@ struct artea_gpu_server {
     cudaStream_t kstream = nullptr, cstream = nullptr;
     cudaEvent_t kdone = nullptr;
     bool launched = false;
-    uint32_t* h_closed = nullptr;       // mapped: the running instance closed its ring
+    uint32_t* h_closed = nullptr;       // mapped: the running instance closed its ring (kClosed*)
     uint32_t* d_closed_alias = nullptr;
+    uint32_t* h_beat = nullptr;         // mapped: heartbeat counter advanced by beat_thread
+    uint32_t* d_beat_alias = nullptr;
+    uint32_t beat_limit_ms = 0;
+    std::thread beat_thread;
+    std::mutex beat_mu;
+    std::condition_variable beat_cv;
+    bool beat_quit = false;
+    std::atomic<bool> beat_paused{false};
     // device ring and control
     float* d_q = nullptr;
     uint32_t* d_topk = nullptr;
@@ -219,8 +250,10 @@ int launch_serving(artea_gpu_server* s) {
     c.stop = s->d_ctl + 3;
     c.done = s->d_done_alias;
     c.closed = s->d_closed_alias;
+    c.beat = s->d_beat_alias;
     c.ring = s->ring;
     c.idle_limit = s->idle_limit;
+    c.beat_limit_ms = s->beat_limit_ms;
     CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(s->fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(s->smem)));
     // Reopen the ring (the previous instance closed it before exiting); same
@@ -248,6 +281,9 @@ bool all_done(const artea_gpu_server* s, uint64_t seq0, uint32_t n) {
 // decides, not an event on its stream: the new instance is queued on the same
 // stream and starts once the old one has drained.
 int ensure_running(artea_gpu_server* s) {
+    if (*static_cast<volatile uint32_t*>(s->h_closed) == kClosedHeartbeat)
+        return fail(ARTEA_GPU_ETIMEOUT, "serving kernel ended: the host heartbeat was stale for " +
+                                            std::to_string(s->beat_limit_ms) + " ms; destroy the server");
     if (s->next_seq == s->consumed_upto) return ARTEA_GPU_OK;
     if (s->launched) {
         if (*static_cast<volatile uint32_t*>(s->h_closed) == 0u) return ARTEA_GPU_OK;
@@ -292,11 +328,15 @@ extern "C" int artea_gpu_server_create(artea_gpu_index* ix, const artea_gpu_serv
     s->ring = o.ring_slots;
     s->warps = o.warps_per_cta ? o.warps_per_cta : 2;
     if (s->warps > 8) return cleanup(fail(ARTEA_GPU_EINVAL, "warps_per_cta must be <= 8"));
-    // By default the kernel does not end on idle (it ends at destroy): a kernel
-    // instance that ends and a new one queued behind it on the same stream has
-    // been seen to leave the new one waiting although every warp of the old one
-    // had exited. A positive idle_polls restores the idle exit.
-    s->idle_limit = o.idle_polls ? o.idle_polls : 0xFFFFFFFFu;   // microseconds
+    // The kernel does not end on idle (it ends at destroy, or when the
+    // heartbeat goes stale): an instance that ended and a new one queued behind
+    // it on the same stream was seen to leave the new one waiting although
+    // every warp of the old one had exited, and the cause is not known, so an
+    // idle window is refused.
+    if (o.idle_polls != 0)
+        return cleanup(fail(ARTEA_GPU_EINVAL, "idle_polls must be 0: the idle exit and relaunch are disabled"));
+    s->idle_limit = 0xFFFFFFFFu;
+    s->beat_limit_ms = o.heartbeat_ms ? o.heartbeat_ms : 2000u;
     s->cap = std::max<uint32_t>(2u * s->qmax, 2u);
     uint32_t kb = 1;
     while (kb < 32 && (1ull << kb) < ix->n) ++kb;
@@ -338,20 +378,38 @@ extern "C" int artea_gpu_server_create(artea_gpu_index* ix, const artea_gpu_serv
             cudaSuccess ||
         cudaHostAlloc(reinterpret_cast<void**>(&s->h_done), sizeof(uint32_t) * s->ring, cudaHostAllocMapped) !=
             cudaSuccess ||
-        cudaHostAlloc(reinterpret_cast<void**>(&s->h_closed), sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess)
+        cudaHostAlloc(reinterpret_cast<void**>(&s->h_closed), sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostAlloc(reinterpret_cast<void**>(&s->h_beat), sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess)
         return cleanup(fail(ARTEA_GPU_ENOMEM, "pinned host allocation failed"));
     std::memset(s->h_done, 0, sizeof(uint32_t) * s->ring);
     *s->h_closed = 0u;
+    *s->h_beat = 0u;
     if (cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_out_alias), s->h_out, 0) != cudaSuccess ||
         cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_done_alias), s->h_done, 0) != cudaSuccess ||
-        cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_closed_alias), s->h_closed, 0) != cudaSuccess)
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_closed_alias), s->h_closed, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_beat_alias), s->h_beat, 0) != cudaSuccess)
         return cleanup(fail(ARTEA_GPU_ECUDA, "mapped host memory unavailable"));
     if (cudaStreamCreateWithFlags(&s->kstream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->kdone, cudaEventDisableTiming) != cudaSuccess)
         return cleanup(fail(ARTEA_GPU_ECUDA, "stream/event creation failed"));
     s->consumed.assign(s->ring, 0);
+    // The heartbeat: advanced 8 times per limit while the server exists.
+    const auto period = std::chrono::milliseconds(std::max<uint32_t>(1u, s->beat_limit_ms / 8u));
+    s->beat_thread = std::thread([s, period] {
+        std::unique_lock<std::mutex> lk(s->beat_mu);
+        while (!s->beat_quit) {
+            if (!s->beat_paused.load()) *static_cast<volatile uint32_t*>(s->h_beat) += 1u;
+            s->beat_cv.wait_for(lk, period);
+        }
+    });
     *out = s;
+    return ARTEA_GPU_OK;
+}
+
+extern "C" int artea_gpu_server_pause_heartbeat(artea_gpu_server* s) {
+    if (!s) return fail(ARTEA_GPU_EINVAL, "null server");
+    s->beat_paused.store(true);
     return ARTEA_GPU_OK;
 }
 
@@ -362,6 +420,7 @@ extern "C" int artea_gpu_server_submit(artea_gpu_server* s, const float* queries
     std::lock_guard<std::mutex> lk(s->mu);
     DeviceGuard guard(s->idx->device);
     if (n > s->ring) return fail(ARTEA_GPU_EINVAL, "request larger than the ring");
+    if (*static_cast<volatile uint32_t*>(s->h_closed) == kClosedHeartbeat) return ensure_running(s);
     if (s->next_seq + n - s->consumed_upto > s->ring) return fail(ARTEA_GPU_EBUSY, "ring full: poll first");
     for (uint32_t i = 0; i < n; ++i) {
         const uint32_t k = topk ? topk[i] : s->kmax;
@@ -423,7 +482,10 @@ extern "C" int artea_gpu_server_poll(artea_gpu_server* s, uint64_t ticket, uint3
         s->consumed_upto++;
     }
     *done = 1;
-    return ensure_running(s);
+    // The request's results are delivered; a stale heartbeat is reported by
+    // the next call that needs the kernel.
+    const int rc = ensure_running(s);
+    return rc == ARTEA_GPU_ETIMEOUT ? ARTEA_GPU_OK : rc;
 }
 
 extern "C" int artea_gpu_server_stats(const artea_gpu_server* s, uint64_t* published, uint64_t* consumed,
@@ -439,6 +501,14 @@ extern "C" int artea_gpu_server_stats(const artea_gpu_server* s, uint64_t* publi
 extern "C" int artea_gpu_server_destroy(artea_gpu_server* s) {
     if (!s) return ARTEA_GPU_OK;
     DeviceGuard guard(s->idx->device);
+    if (s->beat_thread.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(s->beat_mu);
+            s->beat_quit = true;
+        }
+        s->beat_cv.notify_all();
+        s->beat_thread.join();
+    }
     if (s->d_ctl) {
         const uint32_t one = 1;
         cudaMemcpy(s->d_ctl + 3, &one, sizeof(uint32_t), cudaMemcpyHostToDevice);
@@ -457,6 +527,7 @@ extern "C" int artea_gpu_server_destroy(artea_gpu_server* s) {
     if (s->h_out) cudaFreeHost(s->h_out);
     if (s->h_done) cudaFreeHost(s->h_done);
     if (s->h_closed) cudaFreeHost(s->h_closed);
+    if (s->h_beat) cudaFreeHost(s->h_beat);
     if (s->kdone) cudaEventDestroy(s->kdone);
     if (s->kstream) cudaStreamDestroy(s->kstream);
     if (s->cstream) cudaStreamDestroy(s->cstream);

@@ -23,7 +23,7 @@ from .router import DeviceIndex, GpuRouter, metric_code, MODES
 
 class Server:
     def __init__(self, index: DeviceIndex, metric, max_topk: int, max_queue: int, ring_slots: int = 16384,
-                 mode: str = "exact", warps_per_cta: int = 0, idle_polls: int = 0):
+                 mode: str = "exact", warps_per_cta: int = 0, idle_polls: int = 0, heartbeat_ms: int = 0):
         o = nat.ServerOpts()
         o.metric = metric_code(metric)
         o.mode = MODES[mode]
@@ -32,11 +32,18 @@ class Server:
         o.ring_slots = ring_slots
         o.warps_per_cta = warps_per_cta
         o.idle_polls = idle_polls
+        o.heartbeat_ms = heartbeat_ms
         h = ctypes.c_void_p()
         nat.check(nat.lib().artea_gpu_server_create(index.handle, ctypes.byref(o), ctypes.byref(h)))
         self._h = h
         self.index = index
         self.max_topk = max_topk
+
+    def __enter__(self) -> "Server":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
 
     def submit(self, queries: np.ndarray, topk: Optional[np.ndarray] = None,
                queue: Optional[np.ndarray] = None) -> Optional[int]:
@@ -68,6 +75,11 @@ class Server:
                 return r
             if time.perf_counter() - t0 > timeout_s:
                 raise TimeoutError(f"request {ticket} not finished after {timeout_s} s")
+
+    def pause_heartbeat(self) -> None:
+        """Stop the server's heartbeat, as a host that stopped answering would
+        (failure injection: the kernel ends heartbeat_ms later)."""
+        nat.check(nat.lib().artea_gpu_server_pause_heartbeat(self._h))
 
     def stats(self) -> dict:
         p, c, l = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()

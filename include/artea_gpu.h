@@ -147,12 +147,30 @@ typedef struct artea_gpu_router_opts {
                                    0xFFFFFFFF = no table (HBM bitset only) */
     uint32_t register_budget;   /* registers per thread of the persistent kernel:
                                    64 (32 warps per SM), 85 (80 used, 24
-                                   warps) or 96 (20 warps; CTAs of at most 4
-                                   warps); 0 = autotuned */
+                                   warps), 96 (20 warps) or 128 (16 warps;
+                                   96 and 128: CTAs of at most 4 warps);
+                                   0 = autotuned */
     uint32_t stage_rows;        /* persistent kernel's row reads: 8 = each pass's
                                    candidate rows staged in shared memory by TMA
                                    bulk copies; 0xFFFFFFFF = vector loads from
                                    HBM/L2; 0 = autotuned */
+    uint32_t pipeline;          /* level-0 loop: 0 (or 1) = pipelined across
+                                   expansions where every level-0 row holds at
+                                   most 64 distinct ids (the next row is
+                                   collected and its first rows' loads issued
+                                   before the current batch is merged);
+                                   0xFFFFFFFF = one expansion at a time */
+    uint32_t prefetch_rows;     /* neighbour rows whose loads the pipelined loop
+                                   issues ahead of their distance phase: 8 = the
+                                   first pass (into registers with the
+                                   128-register budget, else into L2), 16 = also
+                                   the second pass's rows (into L2);
+                                   0 = autotuned */
+    uint32_t order_queries;     /* persistent schedule with per-query queue
+                                   sizes: 0 = queries are started largest queue
+                                   first (longest work first, so the short
+                                   queries fill the tail), 0xFFFFFFFF = index
+                                   order. Results do not depend on it. */
 } artea_gpu_router_opts;
 
 /* Library / device information. */
@@ -212,9 +230,13 @@ int artea_gpu_batch_query(artea_gpu_router* router, const float* queries, uint32
                           uint32_t k_stride, uint64_t* out_entries, artea_gpu_query_stats* stats);
 
 /* Same on device buffers, enqueued on `stream` (a cudaStream_t; NULL = the
- * CUDA default stream); returns without waiting. Buffers must be 16-byte
- * aligned. Per-query arrays and stats are
- * device pointers or NULL. */
+ * CUDA default stream); returns without waiting, except on the autotuner's
+ * first call: a persistent-schedule router that leaves a launch option to the
+ * autotuner times candidate launches on the first call for each (dim, queue
+ * capacity, batch-size bucket, per-query arrays) it sees that no earlier
+ * process recorded (see artea_gpu_router_opts), on `stream`, and waits for
+ * them, so make that call before any stream capture. Buffers must be 16-byte
+ * aligned. Per-query arrays and stats are device pointers or NULL. */
 int artea_gpu_batch_query_device(artea_gpu_router* router, const float* d_queries, uint32_t nq,
                                  const uint32_t* d_topk, const uint32_t* d_queue, uint32_t k_stride,
                                  uint64_t* d_out, artea_gpu_query_stats* d_stats, void* stream);
@@ -286,6 +308,11 @@ int artea_gpu_router_set_phase_buffer(artea_gpu_router* router, void* d_phase_cy
  * stage_rows 0 = vector loads, 8 = TMA-staged rows. */
 int artea_gpu_router_tuning(const artea_gpu_router* router, uint32_t* warps_per_cta, uint32_t* visited_hash_bits,
                             uint32_t* register_budget, uint32_t* stage_rows);
+/* More of the last launch's parameters: pipelined level-0 loop (0/1),
+ * neighbour rows loaded ahead (8 or 16), queries started largest queue first
+ * (0/1). No reference counterpart (measurement only). */
+int artea_gpu_router_tuning_ext(const artea_gpu_router* router, uint32_t* pipeline, uint32_t* prefetch_rows,
+                                uint32_t* ordered);
 
 /* ---- Serving loop (continuous batching) ----
  * No counterpart in the reference, whose batch_query is one blocking call; each
@@ -297,10 +324,13 @@ int artea_gpu_router_tuning(const artea_gpu_router* router, uint32_t* warps_per_
  * one per warp; queries of requests submitted while others run overlap on the
  * device. poll() reports a request done once all its queries are; it copies
  * their rows out and frees the slots. Idle warps read the ring counters without
- * atomics and back off; with idle_polls set the kernel exits after that many
- * microseconds without work and submit()/poll() relaunch it when work is
- * pending; by default it stays resident (holding the GPU's warp slots) until
- * the server is destroyed. */
+ * atomics and back off. The kernel stays resident (holding the GPU's warp
+ * slots) until the server is destroyed, or until a heartbeat that a thread of
+ * the server advances in mapped host memory has not moved for heartbeat_ms:
+ * then an idle warp closes the ring and the kernel ends, and submit() and
+ * poll() of unfinished work return ARTEA_GPU_ETIMEOUT (destroy the server). So
+ * no wait of the kernel outlives a host that stopped answering by more than
+ * heartbeat_ms. */
 typedef struct artea_gpu_server artea_gpu_server;
 
 typedef struct artea_gpu_server_opts {
@@ -310,8 +340,12 @@ typedef struct artea_gpu_server_opts {
     uint32_t max_queue;      /* largest queue size of any query */
     uint32_t ring_slots;     /* queries in flight (admission limit) */
     uint32_t warps_per_cta;  /* 0 = 2 */
-    uint32_t idle_polls;     /* microseconds idle before the kernel exits; 0 = never
-                                (the kernel stays resident until destroy) */
+    uint32_t idle_polls;     /* must be 0: an idle exit followed by a relaunch on
+                                the same stream was seen to leave the new kernel
+                                unstarted (cause unknown), so it is refused with
+                                ARTEA_GPU_EINVAL */
+    uint32_t heartbeat_ms;   /* the kernel ends once the host heartbeat has not
+                                moved for this long; 0 = 2000 */
 } artea_gpu_server_opts;
 
 int artea_gpu_server_create(artea_gpu_index* index, const artea_gpu_server_opts* opts, artea_gpu_server** out);
@@ -326,6 +360,10 @@ int artea_gpu_server_poll(artea_gpu_server* server, uint64_t ticket, uint32_t n,
 int artea_gpu_server_stats(const artea_gpu_server* server, uint64_t* published, uint64_t* consumed,
                            uint64_t* kernel_launches);
 int artea_gpu_server_destroy(artea_gpu_server* server);
+/* Failure injection on the host: stops this server's heartbeat, as a host
+ * that no longer answers would (the kernel ends heartbeat_ms later and
+ * unfinished work reports ARTEA_GPU_ETIMEOUT). */
+int artea_gpu_server_pause_heartbeat(artea_gpu_server* server);
 
 /* batch_query on device buffers for callers that cannot allocate device
  * memory (inside an allocator callback, under a fully reserved memory pool,

@@ -11,7 +11,8 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-GOLDEN_CASES = ["early_stop_top0", "early_stop_top2", "early_stop_sqr", "axis80", "sift2k", "deep1k_cos", "gist400"]
+GOLDEN_CASES = ["early_stop_top0", "early_stop_top2", "early_stop_sqr", "axis80", "sift2k", "deep1k_cos", "gist400",
+                "repeats"]
 EARLY_STOP_CASES = ["early_stop_top2", "early_stop_sqr", "sift2k", "gist400"]
 BUILDER = os.path.join(ROOT, "index_build", "_ref", "artea_build_index")
 

@@ -9,9 +9,10 @@ Every expected output below comes from the reference's own code: graphs from
 its CPU builder (index_build/_ref/artea_build_index) and query results and
 distance-call counts from its hierarchical_graph_router_t (oracle/_ref). The
 hand-made graphs restate the shapes of the reference's unit tests
-(unit_tests/test_router_early_stop.cpp:59-97 and
-unit_tests/test_compact_csr_query.cpp:20-37); their expected answers are also
-re-derived independently (an exact sort) in the tests.
+(unit_tests/test_router_early_stop.cpp:59-97,
+unit_tests/test_compact_csr_query.cpp:20-37 and, for rows that repeat ids,
+:89-146); the expected answers of the first two are also re-derived
+independently (an exact sort) in the tests.
 """
 
 from __future__ import annotations
@@ -80,6 +81,60 @@ def axis_queries() -> np.ndarray:
     q = np.zeros((5, 128), dtype=np.float32)
     q[:, 0] = [-2.0, 12.25, 39.5, 60.75, 90.0]
     return q
+
+
+REPEAT_ROW = [2, 0, 3, 3, 1, 5, 7, 5, 4, 6, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18]
+
+
+def repeats_graph(n: int = 320, seed: int = 23):
+    """Rows that name ids more than once and ids already visited, restating at
+    graph scale what unit_tests/test_compact_csr_query.cpp:89-146 pins for
+    process_prefetched_neighbors: a later occurrence of an id in the row, and
+    an id visited before the row is read, are skipped; ids are marked visited
+    when collected. Vertex 20's level-0 row is that test's row; 0, 1 and 20
+    open the entry vertex's level-0 row. Other level-0 rows are each vertex's
+    nearest vertices with repeats, the vertex itself and the entry point mixed
+    in; some are longer than 64 ids (bl 96), so the collect loop takes them in
+    several chunks. Level-1 rows repeat ids too. Integer-valued vectors give
+    many equal distances. Returns (graph, base, queries)."""
+    rng = np.random.default_rng(seed)
+    dim = 16
+    base = rng.integers(0, 6, size=(n, dim)).astype(np.float32)
+    queries = rng.integers(0, 6, size=(40, dim)).astype(np.float32)
+    entry = 21
+    hl = [0] * n
+    lvl1 = sorted(set([entry, 20] + rng.choice(n, 30, replace=False).tolist()))
+    for v in lvl1:
+        hl[v] = 1
+    d2 = ((base[:, None, :] - base[None, :, :]) ** 2).sum(-1)
+    rows = []
+    for v in range(n):
+        r = {}
+        order = [int(u) for u in np.argsort(d2[v], kind="stable") if u != v]
+        k = int(rng.integers(6, 40))
+        row = order[:k]
+        for _ in range(int(rng.integers(1, 12))):                    # repeats, adjacent or later
+            pos = int(rng.integers(0, len(row) + 1))
+            row.insert(pos, row[int(rng.integers(0, len(row)))])
+        if rng.random() < 0.5:
+            row.insert(int(rng.integers(0, len(row) + 1)), v)          # the vertex itself (visited)
+        if rng.random() < 0.5:
+            row.insert(int(rng.integers(0, len(row) + 1)), entry)      # the entry point
+        if rng.random() < 0.15:
+            row = (row * 3)[: int(rng.integers(65, 97))]               # longer than 64, repeats
+        r[0] = row[:96]
+        if hl[v] == 1:
+            others = [u for u in lvl1 if u != v]
+            up = [int(u) for u in rng.choice(others, int(rng.integers(3, 12)), replace=False)]
+            up = up + up[: int(rng.integers(0, len(up) + 1))]
+            rng.shuffle(up)
+            r[1] = up[:40]
+        rows.append(r)
+    rows[20][0] = list(REPEAT_ROW)
+    rows[entry][0] = [0, 1, 20] + [u for u in rows[entry][0] if u not in (0, 1, 20)][:40]
+    g = CompactHierarchicalGraph.from_rows(n, hl, rows, entry_point_vid=entry, ul_max_nbr_size=40,
+                                           bl_max_nbr_size=96, top_level=1)
+    return g, base, queries
 
 
 def build_graph(base: np.ndarray, metric: str, workdir: str, **params) -> str:
@@ -236,6 +291,10 @@ def main() -> None:
     if "--early-stop-only" in sys.argv:
         early_stop_fixtures()
         return
+    if "--repeats-only" in sys.argv:
+        g, base, queries = repeats_graph()
+        save_case("repeats", g, base, queries, metric=0, topk=10, queues=[10, 32, 100], l0_only=True)
+        return
     # Hand-made graphs from the reference unit tests.
     for top in (0, 2):
         save_case(f"early_stop_top{top}", early_stop_graph(top), early_stop_vectors(), early_stop_vectors(),
@@ -247,6 +306,8 @@ def main() -> None:
     built_case("sift2k", "sift100k", 2000, 64, "euclidean", 0, 10, [10, 32, 100], quantize_u8=True)
     built_case("deep1k_cos", "deep10m", 1000, 48, "cosine", 2, 10, [16, 64])
     built_case("gist400", "gist1m", 400, 24, "euclidean", 0, 10, [20, 50], l0=0.05)
+    g, base, queries = repeats_graph()
+    save_case("repeats", g, base, queries, metric=0, topk=10, queues=[10, 32, 100], l0_only=True)
     early_stop_fixtures()
     bruteforce_fixtures()
 

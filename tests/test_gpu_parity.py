@@ -62,7 +62,7 @@ def test_exact_counters_match_oracle(name):
     np.testing.assert_array_equal(st[:, :7], ost[:, :7])
 
 
-@pytest.mark.parametrize("name", ["sift2k", "deep1k_cos", "gist400"])
+@pytest.mark.parametrize("name", ["sift2k", "deep1k_cos", "gist400", "repeats"])
 def test_l0_only_matches_reference(name):
     c = golden_case(name)
     idx = index_for(name)
@@ -83,6 +83,28 @@ def test_drop_in_router_surface_matches_reference():
     one = router.query(c.queries[5], c.graph)
     np.testing.assert_array_equal(one, c.words[32][5])
     router.close()
+
+
+@pytest.mark.parametrize("schedule", ["plain", "persistent"])
+def test_repeated_and_previsited_ids_in_rows(schedule):
+    # Level-0 and level-1 rows that repeat ids and name visited ids (the
+    # vertex itself, the entry point, ids collected from earlier rows),
+    # including rows longer than 64 ids: the reference skips a later
+    # occurrence and a visited id and marks ids at collection
+    # (unit_tests/test_compact_csr_query.cpp:89-146). The index must take the
+    # repeated-id path (whole-row collection and the pipelined loop need rows
+    # of distinct ids) and return the reference's words and distance calls.
+    c = golden_case("repeats")
+    idx = index_for("repeats")
+    assert max(len(c.graph.fetch_level_nbrs(v, 0)) for v in range(c.graph.num_vertices)) > 64
+    for L in c.queues:
+        for stage in ((0xFFFFFFFF, 8) if schedule == "persistent" else (0,)):
+            r = GpuRouter(idx, c.metric, c.topk, L, mode="exact", schedule=schedule, stage_rows=stage)
+            out, st = r.batch_query(c.queries, stats=True)
+            np.testing.assert_array_equal(out, c.words[L], err_msg=f"L={L} {schedule} stage={stage}")
+            np.testing.assert_array_equal(st[:, 0].astype(np.uint64), c.calls[L])
+            assert r.tuning()["pipeline"] == 0, "rows with repeated ids must not take the pipelined loop"
+            r.close()
 
 
 def _fast_agreement(exact, fast):
@@ -207,8 +229,9 @@ def test_exact_with_visited_hash_spill_and_register_budgets(sift20k, vh_bits, re
         np.testing.assert_array_equal(out, ref, err_msg=f"vh_bits={vh_bits} regs={regs} warps={warps}")
         if vh_bits == 6:
             assert (st[:, 7] > 0).all(), "expected every query to spill to the bitset"
-        assert r.tuning() == {"warps_per_cta": warps, "visited_hash_bits": vh_bits, "register_budget": regs,
-                              "stage_rows": 0}
+        t = r.tuning()
+        assert {k: t[k] for k in ("warps_per_cta", "visited_hash_bits", "register_budget", "stage_rows")} == \
+            {"warps_per_cta": warps, "visited_hash_bits": vh_bits, "register_budget": regs, "stage_rows": 0}
 
 
 @pytest.mark.parametrize("regs", [64, 85, 96])

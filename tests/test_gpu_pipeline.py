@@ -1,0 +1,131 @@
+"""GPU parity of the pipelined level-0 loop and the persistent schedule's
+query order.
+
+The pipelined loop decides the next expansion as soon as the current batch's
+acceptance is known (the smaller of the first unexplored entry and the
+smallest accepted candidate), collects that row and issues its loads before
+the current batch is merged. It must return the reference's words, distances
+and work counters exactly: here against the one-expansion-at-a-time loop, the
+oracle and the golden fixtures, for every register budget (the 128-register
+kernel holds the next rows in registers, the others prefetch them into L2),
+both prefetch widths, and with queries started largest queue first or in
+index order."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import BUILDER, build_graph, golden_case
+from artea_b200 import datasets as ds
+from artea_b200.graph import CompactHierarchicalGraph
+from artea_b200.router import DeviceIndex, GpuRouter
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+OFF = 0xFFFFFFFF
+
+
+@pytest.fixture(scope="module")
+def sift20k():
+    if not os.path.exists(BUILDER):
+        pytest.skip("index builder not built")
+    w = ds.WORKLOADS["sift100k"].scaled(20000, 512)
+    base, queries = ds.generate(w)
+    with tempfile.TemporaryDirectory() as tmp:
+        g = CompactHierarchicalGraph.from_hgra(build_graph(base, "euclidean", tmp))
+    return g, base, queries
+
+
+@pytest.fixture(scope="module")
+def uneven_ref(sift20k):
+    g, base, queries = sift20k
+    nq = queries.shape[0]
+    rng = np.random.default_rng(17)
+    topk = rng.choice(np.array([10, 100], np.uint32), nq)
+    queue = np.maximum(rng.choice(np.array([64, 128, 256, 512], np.uint32), nq), topk)
+    ref, ost = orc.batch_query(g, base, queries, topk, queue, metric=0, k_stride=100, stats=True)
+    return topk, queue, ref, ost
+
+
+@pytest.mark.parametrize("regs,warps", [(96, 4), (128, 4), (128, 2), (85, 8), (64, 8)])
+@pytest.mark.parametrize("prefetch", [8, 16])
+def test_pipelined_loop_matches_oracle(sift20k, uneven_ref, regs, warps, prefetch):
+    g, base, queries = sift20k
+    topk, queue, ref, ost = uneven_ref
+    idx = DeviceIndex(g, base)
+    r = GpuRouter(idx, 0, 100, 512, mode="exact", schedule="persistent", warps_per_cta=warps, visited_hash_bits=9,
+                  register_budget=regs, stage_rows=OFF, prefetch_rows=prefetch)
+    out, st = r.batch_query(queries, topk=topk, queue=queue, k_stride=100, stats=True)
+    np.testing.assert_array_equal(out, ref, err_msg=f"regs={regs} warps={warps} prefetch={prefetch}")
+    np.testing.assert_array_equal(st[:, :7], ost[:, :7])
+    t = r.tuning()
+    assert t["pipeline"] == 1 and t["prefetch_rows"] == prefetch and t["register_budget"] == regs
+    assert t["ordered"] == 1, "per-query queue sizes: largest queue first by default"
+    r.close()
+    idx.close()
+
+
+@pytest.mark.parametrize("schedule", ["plain", "persistent"])
+def test_pipelined_equals_one_expansion_loop(sift20k, schedule):
+    g, base, queries = sift20k
+    idx = DeviceIndex(g, base)
+    outs = {}
+    for pipe in (0, OFF):
+        r = GpuRouter(idx, 0, 100, 200, mode="exact", schedule=schedule, pipeline=pipe, stage_rows=OFF)
+        outs[pipe] = r.batch_query(queries, stats=True)
+        assert r.tuning()["pipeline"] == (1 if pipe == 0 else 0)
+        r.close()
+    np.testing.assert_array_equal(outs[0][0], outs[OFF][0])
+    np.testing.assert_array_equal(outs[0][1][:, :7], outs[OFF][1][:, :7])
+    np.testing.assert_array_equal(outs[0][0], orc.batch_query(g, base, queries, 100, 200, metric=0))
+    idx.close()
+
+
+def test_query_order_does_not_change_results(sift20k, uneven_ref):
+    g, base, queries = sift20k
+    topk, queue, ref, _ = uneven_ref
+    idx = DeviceIndex(g, base)
+    for order in (0, OFF):
+        for graphs in (False, True):
+            r = GpuRouter(idx, 0, 100, 512, mode="exact", schedule="persistent", order_queries=order,
+                          use_graphs=graphs, warps_per_cta=2, visited_hash_bits=9, register_budget=96,
+                          stage_rows=OFF, prefetch_rows=8)
+            for _ in range(2):
+                out = r.batch_query(queries, topk=topk, queue=queue, k_stride=100)
+                np.testing.assert_array_equal(out, ref, err_msg=f"order={order} graphs={graphs}")
+            assert r.tuning()["ordered"] == (1 if order == 0 else 0)
+            r.close()
+    idx.close()
+
+
+@pytest.mark.parametrize("name", ["sift2k", "deep1k_cos", "gist400"])
+@pytest.mark.parametrize("regs", [96, 128])
+def test_pipelined_loop_matches_reference_fixtures(name, regs):
+    c = golden_case(name)
+    idx = DeviceIndex(c.graph, c.base)
+    for L in c.queues:
+        for prefetch in (8, 16):
+            r = GpuRouter(idx, c.metric, c.topk, L, mode="exact", schedule="persistent", warps_per_cta=2,
+                          visited_hash_bits=8, register_budget=regs, stage_rows=OFF, prefetch_rows=prefetch)
+            out, st = r.batch_query(c.queries, stats=True)
+            np.testing.assert_array_equal(out, c.words[L], err_msg=f"{name} L={L} regs={regs} pf={prefetch}")
+            np.testing.assert_array_equal(st[:, 0].astype(np.uint64), c.calls[L])
+            assert r.tuning()["pipeline"] == 1
+            r.close()
+    idx.close()
+
+
+def test_fast_mode_pipelined_within_tolerance(sift20k):
+    # FAST mode takes the same pipelined loop; it must agree with EXACT on
+    # >= 99.9% of top-k ids.
+    g, base, queries = sift20k
+    idx = DeviceIndex(g, base)
+    ex = GpuRouter(idx, 0, 100, 200, mode="exact", register_budget=128, stage_rows=OFF).batch_query(queries)
+    fa = GpuRouter(idx, 0, 100, 200, mode="fast", register_budget=128, stage_rows=OFF).batch_query(queries)
+    ev = (ex & np.uint64(0x7FFFFFFF)).astype(np.int64)
+    fv = (fa & np.uint64(0x7FFFFFFF)).astype(np.int64)
+    agree = sum(len(set(a) & set(b)) for a, b in zip(ev, fv)) / ev.size
+    assert agree >= 0.999
+    idx.close()

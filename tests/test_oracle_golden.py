@@ -15,7 +15,7 @@ def test_oracle_matches_reference_words_and_calls(name):
         np.testing.assert_array_equal(st[:, 0].astype(np.uint64), c.calls[L], err_msg=f"{name} L={L} calls")
 
 
-@pytest.mark.parametrize("name", [n for n in GOLDEN_CASES if n in ("sift2k", "deep1k_cos", "gist400")])
+@pytest.mark.parametrize("name", [n for n in GOLDEN_CASES if n in ("sift2k", "deep1k_cos", "gist400", "repeats")])
 def test_oracle_l0_only_matches_reference(name):
     c = golden_case(name)
     for L in c.queues:
