@@ -82,6 +82,7 @@ class RouterOpts(ctypes.Structure):
         ("pipeline", c_uint32),
         ("prefetch_rows", c_uint32),
         ("order_queries", c_uint32),
+        ("warps_per_query", c_uint32),
     ]
 
 
@@ -138,7 +139,8 @@ SIGNATURES = {
                                               c_void_p, c_void_p]),
     "artea_gpu_router_tuning": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32),
                                         POINTER(c_uint32)]),
-    "artea_gpu_router_tuning_ext": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32)]),
+    "artea_gpu_router_tuning_ext": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32),
+                                            POINTER(c_uint32)]),
 }
 
 

@@ -48,11 +48,15 @@ struct Tuning {
     uint32_t regs = 0;   // 0: 85-register budget, 1: 64, 2: 96, 3: 128 (96 and 128: CTAs of at most 4 warps)
     uint32_t stage = 0;  // 0: rows read with vector loads; kStageRows: TMA-staged in shared memory
     uint32_t pf = 0;     // pipelined level-0 loop: 1 = the second pass's rows are prefetched into L2
+    uint32_t pipe = 1;   // pipelined level-0 loop where the graph allows it (0: one expansion at a time)
+    uint32_t wpq = 1;    // warps per query: > 1 = cooperative kernel, a CTA of wpq warps per query
 };
 
 // One field per tuning component (graph keys, the launch-shape cache).
 uint64_t tuning_bits(const Tuning& t) {
-    return (static_cast<uint64_t>(t.warps) << 32) | (static_cast<uint64_t>(t.pf) << 28) |
+    return (static_cast<uint64_t>(t.wpq) << 40) | (static_cast<uint64_t>(t.warps) << 32) |
+           (static_cast<uint64_t>(t.pipe) << 29) |
+           (static_cast<uint64_t>(t.pf) << 28) |
            (static_cast<uint64_t>(t.stage) << 24) | (static_cast<uint64_t>(t.vh_bits) << 8) |
            static_cast<uint64_t>(t.regs);
 }
@@ -76,7 +80,7 @@ struct artea_gpu_router {
     uint32_t topk = 0, queue = 0, max_queue = 0, cap = 0, max_batch = 0;
     int metric = 0, mode = 0, schedule = 0;
     uint32_t want_warps = 0, want_ctas_per_sm = 0, want_vh_bits = 0, want_regs = 0, want_stage = 0;
-    uint32_t want_pipeline = 0, want_prefetch = 0, want_order = 0;
+    uint32_t want_pipeline = 0, want_prefetch = 0, want_order = 0, want_wpq = 0;
     bool use_graphs = false;
     cudaStream_t stream = nullptr;
     int num_sms = 0;
@@ -186,19 +190,26 @@ using KernelFn = void (*)(SearchArgs);
 // regs: 0 = 85-register budget (80 registers, 24 warps per SM), 1 = 64,
 // 2 = 96 (CTAs of at most 4 warps) (persistent only); stage: rows staged in
 // shared memory by TMA.
+// Kernels with the pipelined level-0 loop exist for the 96- and 128-register
+// budgets (the 128-register kernel always carries it; it falls back to one
+// expansion at a time on graphs that do not allow it); the others run one
+// expansion at a time.
 template <int kMetric, bool kExact, bool kStage>
-KernelFn pick_persistent_s(uint32_t regs) {
+KernelFn pick_persistent_s(uint32_t regs, bool pipe) {
     switch (regs) {
         case 1: return search_persistent_kernel<kMetric, kExact, 64, kStage>;
-        case 2: return search_persistent_kernel<kMetric, kExact, 96, kStage>;
-        case 3: return kStage ? nullptr : search_persistent_kernel<kMetric, kExact, 128, false>;
+        case 2:
+            if (pipe) return kStage ? nullptr : search_persistent_kernel<kMetric, kExact, 96, false, true>;
+            return search_persistent_kernel<kMetric, kExact, 96, kStage>;
+        case 3: return kStage ? nullptr : search_persistent_kernel<kMetric, kExact, 128, false, true>;
         default: return search_persistent_kernel<kMetric, kExact, 85, kStage>;
     }
 }
 
 template <int kMetric, bool kExact>
-KernelFn pick_persistent(uint32_t regs, bool stage) {
-    return stage ? pick_persistent_s<kMetric, kExact, true>(regs) : pick_persistent_s<kMetric, kExact, false>(regs);
+KernelFn pick_persistent(uint32_t regs, bool stage, bool pipe) {
+    return stage ? pick_persistent_s<kMetric, kExact, true>(regs, pipe)
+                 : pick_persistent_s<kMetric, kExact, false>(regs, pipe);
 }
 
 // Router option register_budget (64, 85, 96, 128) <-> Tuning::regs (1, 0, 2, 3).
@@ -210,17 +221,37 @@ uint32_t regs_budget(uint32_t index) {
 }
 
 template <int kMetric>
-KernelFn pick_kernel_m(bool exact, bool persistent, uint32_t regs, bool stage) {
-    if (persistent) return exact ? pick_persistent<kMetric, true>(regs, stage) : pick_persistent<kMetric, false>(regs, stage);
-    return exact ? search_plain_kernel<kMetric, true> : search_plain_kernel<kMetric, false>;
+KernelFn pick_kernel_m(bool exact, bool persistent, uint32_t regs, bool stage, bool pipe) {
+    if (persistent)
+        return exact ? pick_persistent<kMetric, true>(regs, stage, pipe) : pick_persistent<kMetric, false>(regs, stage, pipe);
+    if (pipe) return exact ? search_plain_kernel<kMetric, true, true> : search_plain_kernel<kMetric, false, true>;
+    return exact ? search_plain_kernel<kMetric, true, false> : search_plain_kernel<kMetric, false, false>;
 }
 
-KernelFn pick_kernel(int metric, bool exact, bool persistent, uint32_t regs = 0, bool stage = false) {
+template <int kMetric>
+KernelFn pick_coop_m(bool exact, uint32_t wpq) {
+    if (wpq == 2) return exact ? search_coop_kernel<kMetric, true, 2> : search_coop_kernel<kMetric, false, 2>;
+    if (wpq == 4) return exact ? search_coop_kernel<kMetric, true, 4> : search_coop_kernel<kMetric, false, 4>;
+    return nullptr;
+}
+
+KernelFn pick_coop(int metric, bool exact, uint32_t wpq) {
     switch (metric) {
-        case ARTEA_GPU_EUCLIDEAN_SQR: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN_SQR>(exact, persistent, regs, stage);
-        case ARTEA_GPU_EUCLIDEAN: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN>(exact, persistent, regs, stage);
-        case ARTEA_GPU_COSINE: return pick_kernel_m<ARTEA_GPU_COSINE>(exact, persistent, regs, stage);
-        case ARTEA_GPU_DOT: return pick_kernel_m<ARTEA_GPU_DOT>(exact, persistent, regs, stage);
+        case ARTEA_GPU_EUCLIDEAN_SQR: return pick_coop_m<ARTEA_GPU_EUCLIDEAN_SQR>(exact, wpq);
+        case ARTEA_GPU_EUCLIDEAN: return pick_coop_m<ARTEA_GPU_EUCLIDEAN>(exact, wpq);
+        case ARTEA_GPU_COSINE: return pick_coop_m<ARTEA_GPU_COSINE>(exact, wpq);
+        case ARTEA_GPU_DOT: return pick_coop_m<ARTEA_GPU_DOT>(exact, wpq);
+        default: return nullptr;
+    }
+}
+
+KernelFn pick_kernel(int metric, bool exact, bool persistent, uint32_t regs = 0, bool stage = false,
+                     bool pipe = false) {
+    switch (metric) {
+        case ARTEA_GPU_EUCLIDEAN_SQR: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN_SQR>(exact, persistent, regs, stage, pipe);
+        case ARTEA_GPU_EUCLIDEAN: return pick_kernel_m<ARTEA_GPU_EUCLIDEAN>(exact, persistent, regs, stage, pipe);
+        case ARTEA_GPU_COSINE: return pick_kernel_m<ARTEA_GPU_COSINE>(exact, persistent, regs, stage, pipe);
+        case ARTEA_GPU_DOT: return pick_kernel_m<ARTEA_GPU_DOT>(exact, persistent, regs, stage, pipe);
         default: return nullptr;
     }
 }
@@ -284,20 +315,27 @@ int persistent_shape(artea_gpu_router* r, const Tuning& t, LaunchShape* s) {
     }
     if ((t.regs == 2 || t.regs == 3) && t.warps > 4)
         return fail(ARTEA_GPU_EINVAL, "register budgets 96 and 128 allow at most 4 warps per CTA");
-    KernelFn fn = pick_kernel(r->metric, r->mode == ARTEA_GPU_MODE_EXACT, true, t.regs, t.stage != 0);
-    if (!fn) return fail(ARTEA_GPU_EINVAL, "no kernel for this combination (staged rows with the 128-register budget)");
-    const uint32_t smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits, t.stage) * t.warps;
+    const bool coop = t.wpq > 1;
+    KernelFn fn = coop ? pick_coop(r->metric, r->mode == ARTEA_GPU_MODE_EXACT, t.wpq)
+                       : pick_kernel(r->metric, r->mode == ARTEA_GPU_MODE_EXACT, true, t.regs, t.stage != 0,
+                                     t.pipe != 0);
+    if (!fn)
+        return fail(ARTEA_GPU_EINVAL, "no kernel for this combination (staged rows with the 128-register budget, or "
+                                      "the pipelined loop with a budget below 96)");
+    const uint32_t cta_threads = coop ? t.wpq * 32 : t.warps * 32;
+    const uint32_t smem = coop ? smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) + kCoopWords * 4
+                               : smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits, t.stage) * t.warps;
     if (smem > 227u * 1024u) return fail(ARTEA_GPU_EINVAL, "persistent CTA needs more than 227 KB shared memory");
     CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(fn),
-                                                           static_cast<int>(t.warps * 32), smem));
+                                                           static_cast<int>(cta_threads), smem));
     if (per_sm <= 0) return fail(ARTEA_GPU_EINVAL, "persistent kernel does not fit on an SM (queue too large?)");
     if (r->want_ctas_per_sm) per_sm = std::min<int>(per_sm, static_cast<int>(r->want_ctas_per_sm));
-    s->warps_per_cta = t.warps;
+    s->warps_per_cta = coop ? t.wpq : t.warps;
     s->ctas = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(r->num_sms);
-    s->slots = s->ctas * t.warps;
+    s->slots = coop ? s->ctas : s->ctas * t.warps;   // one visited slot per search in flight
     r->shapes[key] = *s;
     return ARTEA_GPU_OK;
 }
@@ -337,7 +375,8 @@ int fill_args(artea_gpu_router* r, SearchArgs* a, const float* d_q, uint32_t nq,
     a->phase_cycles = r->d_phase;
     a->early_stop = r->early_stop ? 1u : 0u;
     for (int h = 0; h < kMaxGroups; ++h) a->es_thr[h] = r->es_thr[h];
-    // The pipelined level-0 loop takes whole rows of distinct ids, <= 64 each.
+    // The pipelined level-0 loop takes whole rows of distinct ids, <= 64 each
+    // (prepare_launch applies the launch's tuning on top).
     a->l0_pipe = (r->want_pipeline != kNoHash && ix->l0_unique && ix->bl <= 64u) ? 1u : 0u;
     return ARTEA_GPU_OK;
 }
@@ -357,7 +396,17 @@ struct Prepared {
 
 int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning& t, Prepared* p) {
     const bool exact = r->mode == ARTEA_GPU_MODE_EXACT;
-    KernelFn fn = pick_kernel(r->metric, exact, persistent, t.regs, persistent && t.stage != 0);
+    const bool coop = persistent && t.wpq > 1;
+    // The pipelined loop runs where the graph allows it, the router and the
+    // tuning ask for it, and the kernel carries it (persistent: the 96- and
+    // 128-register kernels with vector loads; the 128-register kernel always
+    // carries it and falls back on its own).
+    const bool staged = persistent && t.stage != 0;
+    const bool has_pipe = !coop && !staged && (persistent ? t.regs == 2 || t.regs == 3 : true);
+    a.l0_pipe = (a.l0_pipe && t.pipe && has_pipe) ? 1u : 0u;
+    const bool pipe_kernel = a.l0_pipe || (persistent && !coop && t.regs == 3);
+    KernelFn fn = coop ? pick_coop(r->metric, exact, t.wpq)
+                       : pick_kernel(r->metric, exact, persistent, t.regs, staged, pipe_kernel);
     if (!fn) return fail(ARTEA_GPU_EINVAL, "no kernel for this metric and option combination");
     a.vh_bits = t.vh_bits;
     {
@@ -370,7 +419,14 @@ int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tun
     }
     p->fn = fn;
     p->persistent = persistent;
-    if (persistent) {
+    if (coop) {
+        LaunchShape s;
+        if (int rc = persistent_shape(r, t, &s)) return rc;
+        p->grid = std::min(s.ctas, a.nq);
+        p->threads = t.wpq * 32;
+        p->smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) + kCoopWords * 4;
+        if (int rc = ensure_slots(r, p->grid)) return rc;
+    } else if (persistent) {
         LaunchShape s;
         if (int rc = persistent_shape(r, t, &s)) return rc;
         const uint32_t needed_ctas = (a.nq + t.warps - 1) / t.warps;
@@ -521,14 +577,17 @@ bool tuning_file_load(const std::string& path, const std::string& fkey, Tuning* 
     bool found = false;
     while (std::fgets(line, sizeof(line), f)) {
         char k[600];
-        unsigned w, b, rg, st, pf;
-        if (std::sscanf(line, "%599s %u %u %u %u %u", k, &w, &b, &rg, &st, &pf) == 6 && fkey == k && rg <= 3 &&
-            (st == 0 || st == kStageRows) && pf <= 1 && w >= 1 && w <= 8 && b <= 12) {
+        unsigned w, b, rg, st, pf, pp, q;
+        if (std::sscanf(line, "%599s %u %u %u %u %u %u %u", k, &w, &b, &rg, &st, &pf, &pp, &q) == 8 && fkey == k &&
+            rg <= 3 && (st == 0 || st == kStageRows) && pf <= 1 && pp <= 1 && w >= 1 && w <= 8 && b <= 12 &&
+            (q == 1 || q == 2 || q == 4)) {
+            t->wpq = q;
             t->warps = w;
             t->vh_bits = b;
             t->regs = rg;
             t->stage = st;
             t->pf = pf;
+            t->pipe = pp;
             found = true;   // the last line for a key wins
         }
     }
@@ -547,7 +606,8 @@ void tuning_file_store(const std::string& path, const std::string& fkey, const T
     }
     FILE* f = std::fopen(path.c_str(), "a");
     if (!f) return;
-    std::fprintf(f, "%s %u %u %u %u %u\n", fkey.c_str(), t.warps, t.vh_bits, t.regs, t.stage, t.pf);
+    std::fprintf(f, "%s %u %u %u %u %u %u %u\n", fkey.c_str(), t.warps, t.vh_bits, t.regs, t.stage, t.pf, t.pipe,
+                 t.wpq);
     std::fclose(f);
 }
 
@@ -559,14 +619,28 @@ uint32_t batch_bucket(uint32_t nq) {
 
 Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     Tuning t;
+    // Whether the pipelined loop is a choice: the graph allows it and the
+    // router leaves it open (pipeline 0); pipeline 1 fixes it on.
+    const bool pipe_open = a.l0_pipe && r->want_pipeline == 0;
     const bool fixed_pf = r->want_prefetch != 0 || !a.l0_pipe;
     const uint32_t pf_fixed = r->want_prefetch == 16 ? 1u : 0u;
-    if (r->want_warps && r->want_vh_bits && r->want_regs && r->want_stage && fixed_pf) {
+    if (r->want_wpq > 1 && r->want_vh_bits) {
+        t.wpq = r->want_wpq;
+        t.warps = 1;
+        t.vh_bits = hash_bits_of(r->want_vh_bits);
+        t.regs = 2;
+        t.stage = 0;
+        t.pf = 0;
+        t.pipe = 0;
+        return t;
+    }
+    if (r->want_wpq <= 1 && r->want_warps && r->want_vh_bits && r->want_regs && r->want_stage && fixed_pf) {
         t.warps = r->want_warps;
         t.vh_bits = hash_bits_of(r->want_vh_bits);
         t.regs = regs_index(r->want_regs);
         t.stage = stage_of(r->want_stage);
         t.pf = pf_fixed;
+        t.pipe = 1;
         return t;
     }
     const uint64_t key = (static_cast<uint64_t>(r->idx->dim) << 40) | (static_cast<uint64_t>(r->cap) << 16) |
@@ -574,7 +648,8 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
                          (a.l0_only ? 1u : 0u);
     auto it = r->tuned.find(key);
     if (it != r->tuned.end()) return it->second;
-    const bool shared = !r->want_warps && !r->want_vh_bits && !r->want_regs && !r->want_stage && !r->want_prefetch;
+    const bool shared = !r->want_warps && !r->want_vh_bits && !r->want_regs && !r->want_stage && !r->want_prefetch &&
+                        !r->want_wpq;
     const std::string path = shared ? tuning_cache_path() : std::string();
     const std::string fkey = shared ? tuning_file_key(r, key) : std::string();
     if (shared && tuning_file_load(path, fkey, &t)) {
@@ -589,6 +664,7 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     if (r->want_regs) reg_choices = {regs_index(r->want_regs)};
     if (r->want_stage) stage_choices = {stage_of(r->want_stage)};
     if (fixed_pf) pf_choices = {pf_fixed};
+    std::vector<uint32_t> pipe_choices = pipe_open ? std::vector<uint32_t>{0, 1} : std::vector<uint32_t>{1};
     cudaEvent_t ev[4];
     for (auto& e : ev) cudaEventCreate(&e);
     float best_ms = 1e30f;
@@ -598,10 +674,17 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     best.regs = reg_choices[0];
     best.stage = stage_choices[0];
     best.pf = pf_choices[0];
+    best.pipe = pipe_choices.back();
     auto time_candidate = [&](const Tuning& c) {
+        if (r->want_wpq && c.wpq != r->want_wpq) return;
         if (c.stage && c.pf) return;           // staged rows use the one-expansion loop
         if (c.stage && c.regs == 3) return;    // no staged 128-register kernel
         if ((c.regs == 2 || c.regs == 3) && c.warps > 4) return;
+        // The 128-register budget exists for the pipelined loop's preloaded
+        // rows; the one-expansion loop only loses warps with it. The
+        // pipelined loop is timed with the 96- and 128-register budgets.
+        if (pipe_open && c.regs == 3 && !c.pipe) return;
+        if (pipe_open && c.pipe && (c.regs == 0 || c.regs == 1)) return;
         LaunchShape s;
         if (persistent_shape(r, c, &s) != ARTEA_GPU_OK) {
             cudaGetLastError();
@@ -629,27 +712,48 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
             best = c;
         }
     };
-    // 1. launch shape, table size and register budget, with vector loads.
-    for (uint32_t reg : reg_choices)
-        for (uint32_t w : warp_choices)
-            for (uint32_t b : bit_choices) {
-                Tuning c;
-                c.warps = w;
-                c.vh_bits = b;
-                c.regs = reg;
-                c.stage = stage_choices[0];
-                c.pf = pf_choices[0];
-                time_candidate(c);
-            }
-    // 2. rows loaded ahead, at the best shape.
-    for (size_t i = 1; i < pf_choices.size(); ++i) {
+    // 1. level-0 loop, launch shape, table size and register budget, with
+    // vector loads.
+    for (uint32_t pipe : pipe_choices)
+        for (uint32_t reg : reg_choices)
+            for (uint32_t w : warp_choices)
+                for (uint32_t b : bit_choices) {
+                    Tuning c;
+                    c.warps = w;
+                    c.vh_bits = b;
+                    c.regs = reg;
+                    c.stage = stage_choices[0];
+                    c.pf = pf_choices[0];
+                    c.pipe = pipe;
+                    time_candidate(c);
+                }
+    // 1b. warps per query: the cooperative kernel (96 registers, vector
+    // loads, one expansion at a time) at every table size.
+    std::vector<uint32_t> wpq_choices = {2, 4};
+    if (r->want_wpq) wpq_choices = r->want_wpq > 1 ? std::vector<uint32_t>{r->want_wpq} : std::vector<uint32_t>{};
+    if (r->want_warps || r->want_regs || r->want_stage || r->want_prefetch || r->want_pipeline == 1)
+        wpq_choices.clear();   // those options describe the one-warp kernels
+    for (uint32_t q : wpq_choices)
+        for (uint32_t b : bit_choices) {
+            Tuning c;
+            c.wpq = q;
+            c.warps = 1;
+            c.vh_bits = b;
+            c.regs = 2;
+            c.stage = 0;
+            c.pf = 0;
+            c.pipe = 0;
+            time_candidate(c);
+        }
+    // 2. rows loaded ahead, at the best shape (pipelined loop only).
+    for (size_t i = 1; i < pf_choices.size() && best.pipe && best.wpq == 1 && a.l0_pipe; ++i) {
         Tuning c = best;
         c.pf = pf_choices[i];
         time_candidate(c);
     }
     // 3. TMA-staged rows at every register budget and warp count, with the
     // best table size found so far.
-    for (size_t i = 1; i < stage_choices.size(); ++i) {
+    for (size_t i = 1; i < stage_choices.size() && r->want_wpq <= 1; ++i) {
         const uint32_t bits = best.vh_bits;
         for (uint32_t reg : reg_choices)
             for (uint32_t w : warp_choices) {
@@ -659,6 +763,7 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
                 c.regs = reg;
                 c.stage = stage_choices[i];
                 c.pf = 0;
+                c.pipe = 0;
                 time_candidate(c);
             }
     }
@@ -907,6 +1012,8 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
         return fail(ARTEA_GPU_EINVAL, "prefetch_rows must be 0 (autotuned), 8 or 16");
     if (o.order_queries != 0 && o.order_queries != 0xffffffffu)
         return fail(ARTEA_GPU_EINVAL, "order_queries must be 0 (largest queue first) or ~0 (index order)");
+    if (o.warps_per_query != 0 && o.warps_per_query != 1 && o.warps_per_query != 2 && o.warps_per_query != 4)
+        return fail(ARTEA_GPU_EINVAL, "warps_per_query must be 0 (autotuned), 1, 2 or 4");
     DeviceGuard guard(ix->device);
     auto* r = new artea_gpu_router();
     r->idx = ix;
@@ -926,6 +1033,7 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
     r->want_pipeline = o.pipeline;
     r->want_prefetch = o.prefetch_rows;
     r->want_order = o.order_queries;
+    r->want_wpq = o.warps_per_query;
     r->use_graphs = o.use_graphs != 0;
     r->words_per_slot = ((static_cast<uint64_t>(ix->n) + 127) / 128) * 4;   // multiple of 4 words
     r->list_cap = std::max<uint32_t>(std::min<uint32_t>(ix->n, 32768), 64);
@@ -1085,11 +1193,13 @@ int artea_gpu_router_tuning(const artea_gpu_router* r, uint32_t* warps_per_cta, 
 }
 
 int artea_gpu_router_tuning_ext(const artea_gpu_router* r, uint32_t* pipeline, uint32_t* prefetch_rows,
-                                uint32_t* ordered) {
-    if (!r || !pipeline || !prefetch_rows || !ordered) return fail(ARTEA_GPU_EINVAL, "null argument");
+                                uint32_t* ordered, uint32_t* warps_per_query) {
+    if (!r || !pipeline || !prefetch_rows || !ordered || !warps_per_query)
+        return fail(ARTEA_GPU_EINVAL, "null argument");
     *pipeline = r->last_pipe ? 1u : 0u;
     *prefetch_rows = r->last.pf ? 16u : 8u;
     *ordered = r->last_ordered ? 1u : 0u;
+    *warps_per_query = r->last.wpq;
     return ARTEA_GPU_OK;
 }
 

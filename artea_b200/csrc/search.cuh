@@ -287,20 +287,27 @@ __device__ __forceinline__ void dist_preload(const DeviceGraph& g, const uint32_
     }
 }
 
-// Distances for cnt candidates (ids in cvid, shared memory) into cdist. With
+// Distances for cnt candidates (ids in cvid, shared memory) into cdist, one
+// pass of 8 rows at a time: passes pass0, pass0 + stride, ... (the warps of a
+// cooperative search split the passes; one warp alone takes them all). With
 // kPre, the first pass's first block of chunks is taken from pre (loaded by
 // dist_preload<true> on the same cvid) instead of being loaded here.
-template <int kMetric, bool kExact, bool kStage, bool kPre = false>
+template <int kMetric, bool kExact, bool kStage, bool kPre = false, bool kSplit = false>
 __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ q, float qsq,
                                 const uint32_t* cvid, float* cdist, uint32_t cnt, Stage& st, int* error,
-                                const ulonglong2 (*pre)[kBlock] = nullptr) {
+                                const ulonglong2 (*pre)[kBlock] = nullptr, uint32_t pass0 = 0,
+                                uint32_t stride = 1) {
+    if (!kSplit) {
+        pass0 = 0;
+        stride = 1;
+    }
     const int lane = lane_id();
     const int r = lane >> 2;
     const int gi = lane & 3;
     const uint32_t dim = g.dim;
     const uint32_t nchunks = dim >> 4;
     const uint32_t sstride = dim + kStagePad;
-    for (uint32_t p = 0; p < cnt; p += 8) {
+    for (uint32_t p = 8u * pass0; p < cnt; p += 8u * stride) {
         const uint32_t idx = p + r;
         const bool valid = idx < cnt;
         const uint32_t vid = valid ? cvid[idx] : 0u;
@@ -364,6 +371,72 @@ __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ 
         if (valid && gi == 0) cdist[idx] = res;
     }
     __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// Cooperative distances (warps per query > 1). A CTA of kW warps searches one
+// query: warp 0 runs the search; at every distance batch it publishes the
+// candidates here and all kW warps take the 8-row passes in turn (warp w:
+// passes w, w + kW, ...), each row by one warp with the same code, so the
+// distances are bit-identical to one warp's. Two named-barrier phases per
+// batch: start (the batch is published) and done (every distance is
+// written). After its last query warp 0 publishes quit at a start barrier.
+// ---------------------------------------------------------------------------
+struct CoopCtl {
+    const uint32_t* cvid;
+    float* cdist;
+    uint32_t cnt;
+    float qsq;
+    uint32_t quit;
+    uint32_t pad[3];
+};
+constexpr uint32_t kCoopWords = sizeof(CoopCtl) / 4;
+constexpr int kCoopBarrier = 1;
+
+__device__ __forceinline__ void coop_barrier(int warps) {
+    asm volatile("barrier.sync %0, %1;" ::"r"(kCoopBarrier), "r"(warps * 32) : "memory");
+}
+
+template <int kMetric, bool kExact, bool kStage, int kW>
+__device__ __forceinline__ void dist_call(const DeviceGraph& g, const float* __restrict__ q, float qsq,
+                                          const uint32_t* cvid, float* cdist, uint32_t cnt, Stage& st, int* error,
+                                          CoopCtl* coop) {
+    if (kW == 1) {
+        batch_distances<kMetric, kExact, kStage>(g, q, qsq, cvid, cdist, cnt, st, error);
+        return;
+    }
+    if (lane_id() == 0) {
+        coop->cvid = cvid;
+        coop->cdist = cdist;
+        coop->cnt = cnt;
+        coop->qsq = qsq;
+        coop->quit = 0u;
+    }
+    coop_barrier(kW);   // start
+    batch_distances<kMetric, kExact, false, false, true>(g, q, qsq, cvid, cdist, cnt, st, error, nullptr, 0u, kW);
+    coop_barrier(kW);   // done
+}
+
+// The other warps of a cooperative CTA: take passes of each published batch
+// until warp 0 publishes quit.
+template <int kMetric, bool kExact, int kW>
+__device__ void coop_helper(const DeviceGraph& g, const float* __restrict__ q, CoopCtl* coop, int warp, int* error) {
+    Stage st;
+    st.buf = nullptr;
+    st.mbar = 0u;
+    st.phase = 0u;
+    for (;;) {
+        coop_barrier(kW);   // start
+        const uint32_t quit = coop->quit;
+        const uint32_t cnt = coop->cnt;
+        const uint32_t* cvid = coop->cvid;
+        float* cdist = coop->cdist;
+        const float qsq = coop->qsq;
+        if (quit) break;
+        batch_distances<kMetric, kExact, false, false, true>(g, q, qsq, cvid, cdist, cnt, st, error, nullptr,
+                                                            static_cast<uint32_t>(warp), kW);
+        coop_barrier(kW);   // done
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1049,6 +1122,7 @@ struct WarpSmem {
     float* bd;
     uint32_t* bv;
     uint32_t* vh;
+    CoopCtl* coop;               // cooperative search's control block (null otherwise)
 };
 
 __device__ __forceinline__ WarpSmem carve(float* base, uint32_t dim, uint32_t cap, uint32_t stage_rows = 0) {
@@ -1064,6 +1138,7 @@ __device__ __forceinline__ WarpSmem carve(float* base, uint32_t dim, uint32_t ca
     s.bd = s.cdist + kCandBatch;
     s.bv = reinterpret_cast<uint32_t*>(s.bd + kCandBatch);
     s.vh = s.bv + kCandBatch;
+    s.coop = nullptr;
     return s;
 }
 
@@ -1205,9 +1280,11 @@ __device__ __forceinline__ void l0_search_pipelined(const SearchArgs& a, Queue& 
 // stage_phase: with kStage, the parity of the next phase of the warp's staging
 // mbarrier, which the caller initialised once (an mbarrier is not initialised
 // again while it is valid) and which carries over from query to query.
-// kRegs: the pipelined level-0 loop holds the next expansion's first pass in
-// registers (the 128-register budget) instead of prefetching it into L2.
-template <int kMetric, bool kExact, bool kStage = false, bool kRegs = false>
+// kPipe: the kernel carries the pipelined level-0 loop (taken when a.l0_pipe;
+// otherwise, and in kernels without it, one expansion at a time). kRegs: the
+// pipelined loop holds the next expansion's first pass in registers (the
+// 128-register budget) instead of prefetching it into L2. kW: warps per query.
+template <int kMetric, bool kExact, bool kStage = false, bool kRegs = false, int kW = 1, bool kPipe = false>
 __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, const WarpSmem& sm,
                            uint32_t* stage_phase = nullptr) {
     const int lane = lane_id();
@@ -1262,7 +1339,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
         uint32_t cur = g.entry;
         if (lane == 0) cvid[0] = cur;
         __syncwarp();
-        batch_distances<kMetric, kExact, kStage>(g, sm.q, qsq, cvid, cdist, 1, st, a.error);
+        dist_call<kMetric, kExact, kStage, kW>(g, sm.q, qsq, cvid, cdist, 1, st, a.error, sm.coop);
         float cur_d = cdist[0];
         ct.dist_evals = 1;
 
@@ -1286,7 +1363,8 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                         collect_unvisited(g, vs, row, len, pos, cvid, &cnt, &consumed, a.error, 0u, 0u, false);
                         pos = consumed;
                         if (cnt == 0) continue;
-                        batch_distances<kMetric, kExact, kStage>(g, sm.q, qsq, cvid, cdist, cnt, st, a.error);
+                        dist_call<kMetric, kExact, kStage, kW>(g, sm.q, qsq, cvid, cdist, cnt, st, a.error,
+                                                               sm.coop);
                         ct.dist_evals += cnt;
                         ct.upper_dist_evals += cnt;
                         // First strict improvement in row order (beam_loop.hpp:153-160).
@@ -1327,7 +1405,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
         q.lb = FLT_MAX;
         queue_insert(q, cur_d, cur, a.error);
         visited_set(vs, cur);
-        if (!kStage && a.l0_pipe) {
+        if (kPipe && !kStage && kW == 1 && a.l0_pipe) {
             l0_search_pipelined<kMetric, kExact, kRegs>(a, q, vs, sm, qsq, cur, ct, pc, st);
         } else {
             // Software pipeline: while one row is processed, the row descriptor and
@@ -1380,7 +1458,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                     pos = consumed;
                     pc.lap(kPhCollect);
                     if (cnt == 0) continue;
-                    batch_distances<kMetric, kExact, kStage>(g, sm.q, qsq, cvid, cdist, cnt, st, a.error);
+                    dist_call<kMetric, kExact, kStage, kW>(g, sm.q, qsq, cvid, cdist, cnt, st, a.error, sm.coop);
                     ct.dist_evals += cnt;
                     pc.lap(kPhDist);
                     if (p2 >= 0 && !pf_have_ids) {
@@ -1438,13 +1516,13 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
 
 // Plain schedule: one CTA of one warp per query; slot = query index
 // (24 resident CTAs per SM at the 85-register budget).
-template <int kMetric, bool kExact>
+template <int kMetric, bool kExact, bool kPipe>
 __global__ void __launch_bounds__(32, 24) search_plain_kernel(SearchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const uint32_t qi = blockIdx.x;
     if (qi >= a.nq) return;
     const WarpSmem sm = carve(smem, a.g.dim, a.cap);
-    search_one<kMetric, kExact>(a, qi, qi, sm);
+    search_one<kMetric, kExact, false, false, 1, kPipe>(a, qi, qi, sm);
 }
 
 // Persistent schedule: warps pull query indices from a shared counter (in
@@ -1459,7 +1537,7 @@ constexpr int budget_min_blocks(int budget) {
     return budget == 64 ? 4 : (budget == 96 ? 5 : (budget == 128 ? 4 : 3));
 }
 
-template <int kMetric, bool kExact, int kBudget, bool kStage = false>
+template <int kMetric, bool kExact, int kBudget, bool kStage = false, bool kPipe = false>
 __global__ void __launch_bounds__(budget_threads(kBudget), budget_min_blocks(kBudget))
     search_persistent_kernel(SearchArgs a) {
     extern __shared__ __align__(16) float smem[];
@@ -1480,12 +1558,41 @@ __global__ void __launch_bounds__(budget_threads(kBudget), budget_min_blocks(kBu
         qi = __shfl_sync(kFull, qi, 0);
         if (qi >= a.nq) break;
         if (a.order) qi = __ldg(a.order + qi);
-        search_one<kMetric, kExact, kStage, kBudget == 128>(a, qi, slot, sm, &stage_phase);
+        search_one<kMetric, kExact, kStage, kBudget == 128, 1, kPipe>(a, qi, slot, sm, &stage_phase);
     }
     if (kStage) {
         __syncwarp();
         if (lane_id() == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(sm.mbar)) : "memory");
     }
+}
+
+// Cooperative persistent schedule: a CTA of kW warps searches one query at a
+// time (queries from the shared counter, in a.order if set); warp 0 runs the
+// search, and every distance batch is split over the kW warps (CoopCtl).
+// Launch bounds give each thread 96 registers. Rows are read with vector
+// loads; the level-0 loop takes one expansion at a time.
+template <int kMetric, bool kExact, int kW>
+__global__ void __launch_bounds__(kW * 32, 20 / kW) search_coop_kernel(SearchArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    const int warp = threadIdx.x >> 5;
+    const uint32_t words = warp_smem_words(a.g.dim, a.cap, a.vh_bits);
+    WarpSmem sm = carve(smem, a.g.dim, a.cap);
+    CoopCtl* coop = reinterpret_cast<CoopCtl*>(smem + words);
+    sm.coop = coop;
+    if (warp != 0) {
+        coop_helper<kMetric, kExact, kW>(a.g, sm.q, coop, warp, a.error);
+        return;
+    }
+    for (;;) {
+        uint32_t qi = 0;
+        if (lane_id() == 0) qi = atomicAdd(a.next_query, 1u);
+        qi = __shfl_sync(kFull, qi, 0);
+        if (qi >= a.nq) break;
+        if (a.order) qi = __ldg(a.order + qi);
+        search_one<kMetric, kExact, false, false, kW>(a, qi, blockIdx.x, sm);
+    }
+    if (lane_id() == 0) coop->quit = 1u;
+    coop_barrier(kW);   // the helpers see quit and leave
 }
 
 }  // namespace artea_gpu

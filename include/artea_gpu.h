@@ -154,12 +154,14 @@ typedef struct artea_gpu_router_opts {
                                    candidate rows staged in shared memory by TMA
                                    bulk copies; 0xFFFFFFFF = vector loads from
                                    HBM/L2; 0 = autotuned */
-    uint32_t pipeline;          /* level-0 loop: 0 (or 1) = pipelined across
-                                   expansions where every level-0 row holds at
-                                   most 64 distinct ids (the next row is
-                                   collected and its first rows' loads issued
-                                   before the current batch is merged);
-                                   0xFFFFFFFF = one expansion at a time */
+    uint32_t pipeline;          /* level-0 loop: 1 = pipelined across expansions
+                                   where every level-0 row holds at most 64
+                                   distinct ids (the next row is collected and
+                                   its first rows' loads issued before the
+                                   current batch is merged); 0xFFFFFFFF = one
+                                   expansion at a time; 0 = autotuned on the
+                                   persistent schedule, pipelined on the plain
+                                   one */
     uint32_t prefetch_rows;     /* neighbour rows whose loads the pipelined loop
                                    issues ahead of their distance phase: 8 = the
                                    first pass (into registers with the
@@ -171,6 +173,12 @@ typedef struct artea_gpu_router_opts {
                                    first (longest work first, so the short
                                    queries fill the tail), 0xFFFFFFFF = index
                                    order. Results do not depend on it. */
+    uint32_t warps_per_query;   /* persistent schedule: 1 = one warp searches a
+                                   query; 2 or 4 = a CTA of that many warps
+                                   searches one query, its distance batches
+                                   split over the warps (for few, long
+                                   searches: small batches, large dims);
+                                   0 = autotuned */
 } artea_gpu_router_opts;
 
 /* Library / device information. */
@@ -310,9 +318,10 @@ int artea_gpu_router_tuning(const artea_gpu_router* router, uint32_t* warps_per_
                             uint32_t* register_budget, uint32_t* stage_rows);
 /* More of the last launch's parameters: pipelined level-0 loop (0/1),
  * neighbour rows loaded ahead (8 or 16), queries started largest queue first
- * (0/1). No reference counterpart (measurement only). */
+ * (0/1), warps per query (1, 2, 4). No reference counterpart (measurement
+ * only). */
 int artea_gpu_router_tuning_ext(const artea_gpu_router* router, uint32_t* pipeline, uint32_t* prefetch_rows,
-                                uint32_t* ordered);
+                                uint32_t* ordered, uint32_t* warps_per_query);
 
 /* ---- Serving loop (continuous batching) ----
  * No counterpart in the reference, whose batch_query is one blocking call; each

@@ -49,7 +49,7 @@ def uneven_ref(sift20k):
     return topk, queue, ref, ost
 
 
-@pytest.mark.parametrize("regs,warps", [(96, 4), (128, 4), (128, 2), (85, 8), (64, 8)])
+@pytest.mark.parametrize("regs,warps", [(96, 4), (96, 2), (128, 4), (128, 2), (128, 1)])
 @pytest.mark.parametrize("prefetch", [8, 16])
 def test_pipelined_loop_matches_oracle(sift20k, uneven_ref, regs, warps, prefetch):
     g, base, queries = sift20k
@@ -72,14 +72,16 @@ def test_pipelined_equals_one_expansion_loop(sift20k, schedule):
     g, base, queries = sift20k
     idx = DeviceIndex(g, base)
     outs = {}
-    for pipe in (0, OFF):
+    for pipe in (1, OFF, 0):
         r = GpuRouter(idx, 0, 100, 200, mode="exact", schedule=schedule, pipeline=pipe, stage_rows=OFF)
         outs[pipe] = r.batch_query(queries, stats=True)
-        assert r.tuning()["pipeline"] == (1 if pipe == 0 else 0)
+        if pipe != 0:
+            assert r.tuning()["pipeline"] == (1 if pipe == 1 else 0)
         r.close()
-    np.testing.assert_array_equal(outs[0][0], outs[OFF][0])
-    np.testing.assert_array_equal(outs[0][1][:, :7], outs[OFF][1][:, :7])
-    np.testing.assert_array_equal(outs[0][0], orc.batch_query(g, base, queries, 100, 200, metric=0))
+    ref = orc.batch_query(g, base, queries, 100, 200, metric=0)
+    for pipe in (1, OFF, 0):   # pipelined, one expansion at a time, autotuned
+        np.testing.assert_array_equal(outs[pipe][0], ref, err_msg=f"pipeline={pipe}")
+        np.testing.assert_array_equal(outs[pipe][1][:, :7], outs[1][1][:, :7])
     idx.close()
 
 
@@ -128,4 +130,63 @@ def test_fast_mode_pipelined_within_tolerance(sift20k):
     fv = (fa & np.uint64(0x7FFFFFFF)).astype(np.int64)
     agree = sum(len(set(a) & set(b)) for a, b in zip(ev, fv)) / ev.size
     assert agree >= 0.999
+    idx.close()
+
+
+# ---------------------------------------------------------------------------
+# Warps per query: a CTA of 2 or 4 warps searches one query, its distance
+# batches split over the warps; words, distances and counters are the
+# reference's.
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("wpq", [2, 4])
+def test_warps_per_query_matches_oracle(sift20k, uneven_ref, wpq):
+    g, base, queries = sift20k
+    topk, queue, ref, ost = uneven_ref
+    idx = DeviceIndex(g, base)
+    for order in (0, OFF):
+        r = GpuRouter(idx, 0, 100, 512, mode="exact", schedule="persistent", warps_per_query=wpq,
+                      visited_hash_bits=9, order_queries=order)
+        out, st = r.batch_query(queries, topk=topk, queue=queue, k_stride=100, stats=True)
+        np.testing.assert_array_equal(out, ref, err_msg=f"warps_per_query={wpq} order={order}")
+        np.testing.assert_array_equal(st[:, :7], ost[:, :7])
+        assert r.tuning()["warps_per_query"] == wpq
+        r.close()
+    idx.close()
+
+
+@pytest.mark.parametrize("name", ["sift2k", "deep1k_cos", "gist400", "repeats", "axis80", "early_stop_top2"])
+@pytest.mark.parametrize("wpq", [2, 4])
+def test_warps_per_query_matches_reference_fixtures(name, wpq):
+    c = golden_case(name)
+    idx = DeviceIndex(c.graph, c.base)
+    for L in c.queues:
+        for graphs in (False, True):
+            r = GpuRouter(idx, c.metric, c.topk, L, mode="exact", schedule="persistent", warps_per_query=wpq,
+                          visited_hash_bits=8, use_graphs=graphs)
+            out, st = r.batch_query(c.queries, stats=True)
+            np.testing.assert_array_equal(out, c.words[L], err_msg=f"{name} L={L} wpq={wpq}")
+            np.testing.assert_array_equal(st[:, 0].astype(np.uint64), c.calls[L])
+            r.close()
+    for cfg, words, calls in c.es:   # enable_early_stop=true fixtures
+        for L in c.queues:
+            r = GpuRouter(idx, c.metric, c.topk, L, mode="exact", schedule="persistent", warps_per_query=wpq,
+                          visited_hash_bits=8)
+            r.set_early_stop(cfg)
+            out, st = r.batch_query(c.queries, stats=True)
+            np.testing.assert_array_equal(out, words[L], err_msg=f"{name} early stop L={L} wpq={wpq}")
+            np.testing.assert_array_equal(st[:, 0].astype(np.uint64), calls[L])
+            r.close()
+    idx.close()
+
+
+def test_autotuner_considers_warps_per_query(sift20k):
+    # A batch of 64 queries leaves most of the GPU idle; whatever the tuner
+    # picks, the words are the oracle's and the pick is reported.
+    g, base, queries = sift20k
+    idx = DeviceIndex(g, base)
+    r = GpuRouter(idx, 0, 100, 200, mode="exact", schedule="persistent")
+    out = r.batch_query(queries[:64])
+    np.testing.assert_array_equal(out, orc.batch_query(g, base, queries[:64], 100, 200, metric=0))
+    assert r.tuning()["warps_per_query"] in (1, 2, 4)
+    r.close()
     idx.close()
