@@ -249,27 +249,47 @@ def profile_traffic(workload: str, tuning: dict, alg_bytes: float, queue=None):
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference's own batch_query on this host's cores.
 # ---------------------------------------------------------------------------
-def cpu_baseline(hgra: str, base: np.ndarray, queries: np.ndarray, topk: int, queue: int, metric: int,
+class CpuReference:
+    """The CPU side of the comparison, opened once per snapshot: the
+    reference's own router (its restore of the HGRA snapshot plus
+    hierarchical_graph_router_t) where it was built and the host has
+    AVX-512, else the C restatement on the host reader's graph."""
+
+    def __init__(self, hgra: str, base: np.ndarray):
+        from oracle import oracle as orc
+        self.orc = orc
+        self.base = base
+        self.ref = orc.RefRouter(hgra, base) if orc.have_ref() and host_has_avx512() else None
+        if self.ref is None:
+            from artea_b200.graph import CompactHierarchicalGraph
+            self.graph = CompactHierarchicalGraph.from_hgra(hgra)
+
+    def close(self):
+        if self.ref is not None:
+            self.ref.close()
+            self.ref = None
+
+
+def cpu_baseline(cpu: CpuReference, queries: np.ndarray, topk: int, queue: int, metric: int,
                  sample: int, repeats: int = 1) -> dict:
     """The reference's batch_query on this host's cores over the first `sample`
     queries; its result words are kept (key "words") for the parity check."""
-    from oracle import oracle as orc
+    orc = cpu.orc
+    base = cpu.base
     q = queries[:sample]
     threads = os.cpu_count() or 1
     words = None
-    if orc.have_ref() and host_has_avx512():
-        r = orc.RefRouter(hgra, base)
+    if cpu.ref is not None:
+        r = cpu.ref
         r.batch_query(q[: min(256, len(q))], topk, queue, metric=metric)   # warm-up
         secs = []
         for _ in range(repeats):
             words, s = r.batch_query(q, topk, queue, metric=metric)
             secs.append(s)
         cores = int(orc.ref_lib().artea_ref_max_threads())
-        r.close()
         kind = "reference"
     else:
-        from artea_b200.graph import CompactHierarchicalGraph
-        g = CompactHierarchicalGraph.from_hgra(hgra)
+        g = cpu.graph
         orc.batch_query(g, base, q[: min(256, len(q))], topk, queue, metric=metric, threads=threads)
         secs = []
         for _ in range(repeats):
@@ -367,21 +387,23 @@ def run_reference_arm(args) -> None:
     metric = metric_code(w.metric)
     sample = min(args.reference_sample or queries.shape[0], queries.shape[0])
     uneven = args.uneven or w.kind == "deep"
+    cpu = CpuReference(hgra, base)
     if uneven:
         # The GPU arm's uneven batch: per-query topk and queue, same draws.
         topk, queue = ds.per_query_params(w, queries.shape[0])
         cfg = {"topk": "per query in {10,100}", "queue": "per query in {64,128,256,512}"}
-        timed = lambda: cpu_baseline_uneven(hgra, base, queries, topk, queue, metric, sample)
+        timed = lambda: cpu_baseline_uneven(cpu, queries, topk, queue, metric, sample)
     else:
         queue, why = reference_queue(args, w, base, queries, hgra, metric)
         cfg = {"topk": w.topk, "queue": queue, "queue_selection": why}
-        timed = lambda: cpu_baseline(hgra, base, queries, w.topk, queue, metric, sample)
+        timed = lambda: cpu_baseline(cpu, queries, w.topk, queue, metric, sample)
     vals = []
     info = None
     for i in range(args.warmup + args.steps):
         info = timed()
         if i >= args.warmup:
             vals.append(info["value"])
+    cpu.close()
     value = statistics.mean(vals)
     line = {"metric": METRIC_NAME, "value": value, "unit": "queries/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sample / value,
@@ -489,7 +511,9 @@ def bench_uneven(args, w, base, queries, hgra, report, index, device, metric, ca
     achieved = alg / (p["ms"] / 1e3) / 1e9
     baseline, par = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        baseline = cpu_baseline_uneven(hgra, base, queries, topk, queue, metric, min(args.cpu_sample or nq, nq))
+        cpu = CpuReference(hgra, base)
+        baseline = cpu_baseline_uneven(cpu, queries, topk, queue, metric, min(args.cpu_sample or nq, nq))
+        cpu.close()
         if args.mode == "exact":
             par = parity(p["words"], baseline["words"], topk[: baseline["words"].shape[0]],
                          against_name(baseline["kind"]))
@@ -529,7 +553,7 @@ def bench_uneven(args, w, base, queries, hgra, report, index, device, metric, ca
     }
 
 
-def cpu_baseline_uneven(hgra, base, queries, topk, queue, metric, sample):
+def cpu_baseline_uneven(cpu, queries, topk, queue, metric, sample):
     """The reference router takes one (topk, queue) per instance: the sample is
     grouped by (topk, queue) and each group runs as one batch_query."""
     groups = {}
@@ -538,7 +562,7 @@ def cpu_baseline_uneven(hgra, base, queries, topk, queue, metric, sample):
     total, info = 0.0, None
     words = np.full((sample, int(topk[:sample].max())), INVALID_WORD, dtype=np.uint64)
     for (k, L), idx in sorted(groups.items()):
-        info = cpu_baseline(hgra, base, queries[idx], k, L, metric, len(idx))
+        info = cpu_baseline(cpu, queries[idx], k, L, metric, len(idx))
         total += info["seconds_per_run"]
         words[np.asarray(idx), :k] = info["words"]
     return {"value": sample / total, "unit": "queries/s", "cores": info["cores"], "kind": info["kind"],
@@ -635,7 +659,9 @@ def bench_fixed(args, w, base, queries, hgra, report, index, device, metric, cac
     traffic, traffic_how = profile_traffic(w.name, tuning, alg_bytes, chosen)
     baseline, par = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        baseline = cpu_baseline(hgra, base, queries, k, chosen, metric, min(args.cpu_sample or nq, nq))
+        cpu = CpuReference(hgra, base)
+        baseline = cpu_baseline(cpu, queries, k, chosen, metric, min(args.cpu_sample or nq, nq))
+        cpu.close()
         if mode == "exact":
             par = parity(words, baseline["words"], k, against_name(baseline["kind"]))
     n_launches = our_launches(router, launches)
