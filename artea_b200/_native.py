@@ -83,6 +83,7 @@ class RouterOpts(ctypes.Structure):
         ("prefetch_rows", c_uint32),
         ("order_queries", c_uint32),
         ("warps_per_query", c_uint32),
+        ("queue_slack", c_uint32),
     ]
 
 
@@ -123,6 +124,7 @@ SIGNATURES = {
     "artea_gpu_batch_query_l0_only": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_void_p, c_void_p]),
     "artea_gpu_router_sync": (c_int, [c_void_p]),
     "artea_gpu_router_launches": (c_int, [c_void_p, POINTER(c_uint64)]),
+    "artea_gpu_router_last_reruns": (c_int, [c_void_p, POINTER(c_uint32)]),
     "artea_gpu_router_set_phase_buffer": (c_int, [c_void_p, c_void_p]),
     "artea_gpu_router_set_early_stop": (c_int, [c_void_p, c_void_p, c_uint32]),
     "artea_gpu_bruteforce": (c_int, [c_void_p, c_int, c_void_p, c_uint32, c_uint32, c_void_p, c_uint32, c_void_p]),
@@ -140,7 +142,7 @@ SIGNATURES = {
     "artea_gpu_router_tuning": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32),
                                         POINTER(c_uint32)]),
     "artea_gpu_router_tuning_ext": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32),
-                                            POINTER(c_uint32)]),
+                                            POINTER(c_uint32), POINTER(c_uint32)]),
 }
 
 

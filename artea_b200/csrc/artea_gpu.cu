@@ -50,11 +50,14 @@ struct Tuning {
     uint32_t pf = 0;     // pipelined level-0 loop: 1 = the second pass's rows are prefetched into L2
     uint32_t pipe = 1;   // pipelined level-0 loop where the graph allows it (0: one expansion at a time)
     uint32_t wpq = 1;    // warps per query: > 1 = cooperative kernel, a CTA of wpq warps per query
+    uint32_t slack = 0;  // queue layout: 0 = 2L entries per search; > 0 = compact, max queue + slack
+                         // entries, a query that could lose a live entry is rerun at 2L
 };
 
 // One field per tuning component (graph keys, the launch-shape cache).
 uint64_t tuning_bits(const Tuning& t) {
-    return (static_cast<uint64_t>(t.wpq) << 40) | (static_cast<uint64_t>(t.warps) << 32) |
+    return (static_cast<uint64_t>(t.slack) << 44) | (static_cast<uint64_t>(t.wpq) << 40) |
+           (static_cast<uint64_t>(t.warps) << 32) |
            (static_cast<uint64_t>(t.pipe) << 29) |
            (static_cast<uint64_t>(t.pf) << 28) |
            (static_cast<uint64_t>(t.stage) << 24) | (static_cast<uint64_t>(t.vh_bits) << 8) |
@@ -80,7 +83,7 @@ struct artea_gpu_router {
     uint32_t topk = 0, queue = 0, max_queue = 0, cap = 0, max_batch = 0;
     int metric = 0, mode = 0, schedule = 0;
     uint32_t want_warps = 0, want_ctas_per_sm = 0, want_vh_bits = 0, want_regs = 0, want_stage = 0;
-    uint32_t want_pipeline = 0, want_prefetch = 0, want_order = 0, want_wpq = 0;
+    uint32_t want_pipeline = 0, want_prefetch = 0, want_order = 0, want_wpq = 0, want_slack = 0;
     bool use_graphs = false;
     cudaStream_t stream = nullptr;
     int num_sms = 0;
@@ -95,6 +98,7 @@ struct artea_gpu_router {
     uint32_t* d_counter = nullptr;
     int* d_error = nullptr;
     uint32_t* d_order = nullptr;   // query order of the persistent schedule (max_batch entries)
+    uint32_t* d_overflow = nullptr;   // compact queues: count, rerun counter, max_batch query indices
 
     // Staging for host-buffer calls.
     float* d_queries = nullptr;
@@ -245,6 +249,20 @@ KernelFn pick_coop(int metric, bool exact, uint32_t wpq) {
     }
 }
 
+KernelFn pick_rerun(int metric, bool exact) {
+    switch (metric) {
+        case ARTEA_GPU_EUCLIDEAN_SQR:
+            return exact ? search_rerun_kernel<ARTEA_GPU_EUCLIDEAN_SQR, true> : search_rerun_kernel<ARTEA_GPU_EUCLIDEAN_SQR, false>;
+        case ARTEA_GPU_EUCLIDEAN:
+            return exact ? search_rerun_kernel<ARTEA_GPU_EUCLIDEAN, true> : search_rerun_kernel<ARTEA_GPU_EUCLIDEAN, false>;
+        case ARTEA_GPU_COSINE:
+            return exact ? search_rerun_kernel<ARTEA_GPU_COSINE, true> : search_rerun_kernel<ARTEA_GPU_COSINE, false>;
+        case ARTEA_GPU_DOT:
+            return exact ? search_rerun_kernel<ARTEA_GPU_DOT, true> : search_rerun_kernel<ARTEA_GPU_DOT, false>;
+        default: return nullptr;
+    }
+}
+
 KernelFn pick_kernel(int metric, bool exact, bool persistent, uint32_t regs = 0, bool stage = false,
                      bool pipe = false) {
     switch (metric) {
@@ -305,6 +323,15 @@ int ensure_stage(artea_gpu_router* r, uint32_t nq, uint32_t k_stride) {
     return ARTEA_GPU_OK;
 }
 
+// The compact queue layout's slack: entries past the largest queue that may
+// hold ties of lb before a search is handed to the full-capacity rerun.
+constexpr uint32_t kCompactSlack = 64;
+
+// Queue entries per search for a tuning point: 2L, or max queue + slack.
+uint32_t launch_cap(const artea_gpu_router* r, const Tuning& t) {
+    return t.slack ? std::max<uint32_t>(r->max_queue + t.slack, 2u) : r->cap;
+}
+
 // Persistent grid for a tuning point: as many CTAs per SM as fit.
 int persistent_shape(artea_gpu_router* r, const Tuning& t, LaunchShape* s) {
     const uint64_t key = tuning_bits(t);
@@ -323,8 +350,9 @@ int persistent_shape(artea_gpu_router* r, const Tuning& t, LaunchShape* s) {
         return fail(ARTEA_GPU_EINVAL, "no kernel for this combination (staged rows with the 128-register budget, or "
                                       "the pipelined loop with a budget below 96)");
     const uint32_t cta_threads = coop ? t.wpq * 32 : t.warps * 32;
-    const uint32_t smem = coop ? smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) + kCoopWords * 4
-                               : smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits, t.stage) * t.warps;
+    const uint32_t cap = launch_cap(r, t);
+    const uint32_t smem = coop ? smem_bytes_per_warp(r->idx->dim, cap, t.vh_bits) + kCoopWords * 4
+                               : smem_bytes_per_warp(r->idx->dim, cap, t.vh_bits, t.stage) * t.warps;
     if (smem > 227u * 1024u) return fail(ARTEA_GPU_EINVAL, "persistent CTA needs more than 227 KB shared memory");
     CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
@@ -392,6 +420,10 @@ struct Prepared {
     bool persistent = false;
     bool order = false;       // run order_by_queue_kernel first (a.order is set)
     SearchArgs a;
+    // Compact queues: the rerun of abandoned queries at 2L (rerun_fn null: none).
+    KernelFn rerun_fn = nullptr;
+    uint32_t rerun_grid = 0, rerun_smem = 0;
+    SearchArgs rerun_a;
 };
 
 int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tuning& t, Prepared* p) {
@@ -408,6 +440,16 @@ int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tun
     KernelFn fn = coop ? pick_coop(r->metric, exact, t.wpq)
                        : pick_kernel(r->metric, exact, persistent, t.regs, staged, pipe_kernel);
     if (!fn) return fail(ARTEA_GPU_EINVAL, "no kernel for this metric and option combination");
+    // The compact queue layout: one-warp persistent kernels only.
+    const bool compact = persistent && !coop && t.slack != 0;
+    a.cap = compact ? launch_cap(r, t) : r->cap;
+    a.compact = compact ? 1u : 0u;
+    if (compact) {
+        if (!r->d_overflow) {
+            if (int rc = dev_alloc(&r->d_overflow, static_cast<size_t>(r->max_batch) + 2)) return rc;
+        }
+        a.overflow = r->d_overflow;
+    }
     a.vh_bits = t.vh_bits;
     {
         uint32_t kb = 1;
@@ -424,7 +466,7 @@ int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tun
         if (int rc = persistent_shape(r, t, &s)) return rc;
         p->grid = std::min(s.ctas, a.nq);
         p->threads = t.wpq * 32;
-        p->smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits) + kCoopWords * 4;
+        p->smem = smem_bytes_per_warp(r->idx->dim, a.cap, t.vh_bits) + kCoopWords * 4;
         if (int rc = ensure_slots(r, p->grid)) return rc;
     } else if (persistent) {
         LaunchShape s;
@@ -432,12 +474,12 @@ int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tun
         const uint32_t needed_ctas = (a.nq + t.warps - 1) / t.warps;
         p->grid = std::min(s.ctas, needed_ctas);
         p->threads = t.warps * 32;
-        p->smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits, t.stage) * t.warps;
+        p->smem = smem_bytes_per_warp(r->idx->dim, a.cap, t.vh_bits, t.stage) * t.warps;
         if (int rc = ensure_slots(r, p->grid * t.warps)) return rc;
     } else {
         p->grid = a.nq;
         p->threads = 32;
-        p->smem = smem_bytes_per_warp(r->idx->dim, r->cap, t.vh_bits);
+        p->smem = smem_bytes_per_warp(r->idx->dim, a.cap, t.vh_bits);
         if (int rc = ensure_slots(r, a.nq)) return rc;
     }
     a.vis_bits = r->d_vis_bits;
@@ -457,6 +499,23 @@ int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tun
     CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(p->smem)));
     p->a = a;
+    if (compact) {
+        // One warp per CTA, the queue at 2L, the HBM bitset as visited set;
+        // slots are the main launch's (it has finished when this starts).
+        SearchArgs b = a;
+        b.cap = r->cap;
+        b.compact = 0;
+        b.vh_bits = 0;
+        b.l0_pipe = 0;
+        b.order = nullptr;
+        p->rerun_a = b;
+        p->rerun_fn = pick_rerun(r->metric, exact);
+        p->rerun_grid = std::min<uint32_t>(r->slots, static_cast<uint32_t>(4 * r->num_sms));
+        p->rerun_smem = smem_bytes_per_warp(r->idx->dim, r->cap, 0);
+        if (!p->rerun_fn) return fail(ARTEA_GPU_EINVAL, "no rerun kernel for this metric");
+        CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(p->rerun_fn),
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p->rerun_smem)));
+    }
     return ARTEA_GPU_OK;
 }
 
@@ -466,8 +525,13 @@ int enqueue(artea_gpu_router* r, const Prepared& p, cudaStream_t st) {
         order_by_queue_kernel<<<1, 1024, 0, st>>>(p.a.queue, p.a.nq, r->d_order);
         CUDA_TRY(cudaGetLastError());
     }
+    if (p.rerun_fn) CUDA_TRY(cudaMemsetAsync(r->d_overflow, 0, 2 * sizeof(uint32_t), st));
     p.fn<<<p.grid, p.threads, p.smem, st>>>(p.a);
     CUDA_TRY(cudaGetLastError());
+    if (p.rerun_fn) {
+        p.rerun_fn<<<p.rerun_grid, 32, p.rerun_smem, st>>>(p.rerun_a);
+        CUDA_TRY(cudaGetLastError());
+    }
     return ARTEA_GPU_OK;
 }
 
@@ -577,11 +641,12 @@ bool tuning_file_load(const std::string& path, const std::string& fkey, Tuning* 
     bool found = false;
     while (std::fgets(line, sizeof(line), f)) {
         char k[600];
-        unsigned w, b, rg, st, pf, pp, q;
-        if (std::sscanf(line, "%599s %u %u %u %u %u %u %u", k, &w, &b, &rg, &st, &pf, &pp, &q) == 8 && fkey == k &&
-            rg <= 3 && (st == 0 || st == kStageRows) && pf <= 1 && pp <= 1 && w >= 1 && w <= 8 && b <= 12 &&
-            (q == 1 || q == 2 || q == 4)) {
+        unsigned w, b, rg, st, pf, pp, q, sl;
+        if (std::sscanf(line, "%599s %u %u %u %u %u %u %u %u", k, &w, &b, &rg, &st, &pf, &pp, &q, &sl) == 9 &&
+            fkey == k && rg <= 3 && (st == 0 || st == kStageRows) && pf <= 1 && pp <= 1 && w >= 1 && w <= 8 &&
+            b <= 12 && (q == 1 || q == 2 || q == 4) && sl <= 4096) {
             t->wpq = q;
+            t->slack = sl;
             t->warps = w;
             t->vh_bits = b;
             t->regs = rg;
@@ -606,8 +671,8 @@ void tuning_file_store(const std::string& path, const std::string& fkey, const T
     }
     FILE* f = std::fopen(path.c_str(), "a");
     if (!f) return;
-    std::fprintf(f, "%s %u %u %u %u %u %u %u\n", fkey.c_str(), t.warps, t.vh_bits, t.regs, t.stage, t.pf, t.pipe,
-                 t.wpq);
+    std::fprintf(f, "%s %u %u %u %u %u %u %u %u\n", fkey.c_str(), t.warps, t.vh_bits, t.regs, t.stage, t.pf, t.pipe,
+                 t.wpq, t.slack);
     std::fclose(f);
 }
 
@@ -634,6 +699,7 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
         t.pipe = 0;
         return t;
     }
+    const uint32_t slack_fixed = (r->want_slack == 0 || r->want_slack == kNoHash) ? 0u : r->want_slack;
     if (r->want_wpq <= 1 && r->want_warps && r->want_vh_bits && r->want_regs && r->want_stage && fixed_pf) {
         t.warps = r->want_warps;
         t.vh_bits = hash_bits_of(r->want_vh_bits);
@@ -641,6 +707,7 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
         t.stage = stage_of(r->want_stage);
         t.pf = pf_fixed;
         t.pipe = 1;
+        t.slack = t.stage ? 0u : slack_fixed;
         return t;
     }
     const uint64_t key = (static_cast<uint64_t>(r->idx->dim) << 40) | (static_cast<uint64_t>(r->cap) << 16) |
@@ -649,7 +716,7 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     auto it = r->tuned.find(key);
     if (it != r->tuned.end()) return it->second;
     const bool shared = !r->want_warps && !r->want_vh_bits && !r->want_regs && !r->want_stage && !r->want_prefetch &&
-                        !r->want_wpq;
+                        !r->want_wpq && !r->want_slack;
     const std::string path = shared ? tuning_cache_path() : std::string();
     const std::string fkey = shared ? tuning_file_key(r, key) : std::string();
     if (shared && tuning_file_load(path, fkey, &t)) {
@@ -665,6 +732,11 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     if (r->want_stage) stage_choices = {stage_of(r->want_stage)};
     if (fixed_pf) pf_choices = {pf_fixed};
     std::vector<uint32_t> pipe_choices = pipe_open ? std::vector<uint32_t>{0, 1} : std::vector<uint32_t>{1};
+    // Queue layout: the compact one pays where the 2L queue is a large part
+    // of a warp's shared memory.
+    std::vector<uint32_t> slack_choices = {0};
+    if (r->want_slack == 0 && r->max_queue >= 128) slack_choices = {0, kCompactSlack};
+    else if (r->want_slack != 0 && r->want_slack != kNoHash) slack_choices = {r->want_slack};
     cudaEvent_t ev[4];
     for (auto& e : ev) cudaEventCreate(&e);
     float best_ms = 1e30f;
@@ -677,6 +749,7 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     best.pipe = pipe_choices.back();
     auto time_candidate = [&](const Tuning& c) {
         if (r->want_wpq && c.wpq != r->want_wpq) return;
+        if (c.slack && (c.wpq > 1 || c.stage)) return;   // compact queues: one-warp kernels, vector loads
         if (c.stage && c.pf) return;           // staged rows use the one-expansion loop
         if (c.stage && c.regs == 3) return;    // no staged 128-register kernel
         if ((c.regs == 2 || c.regs == 3) && c.warps > 4) return;
@@ -714,19 +787,21 @@ Tuning tuned(artea_gpu_router* r, const SearchArgs& a, cudaStream_t st) {
     };
     // 1. level-0 loop, launch shape, table size and register budget, with
     // vector loads.
-    for (uint32_t pipe : pipe_choices)
-        for (uint32_t reg : reg_choices)
-            for (uint32_t w : warp_choices)
-                for (uint32_t b : bit_choices) {
-                    Tuning c;
-                    c.warps = w;
-                    c.vh_bits = b;
-                    c.regs = reg;
-                    c.stage = stage_choices[0];
-                    c.pf = pf_choices[0];
-                    c.pipe = pipe;
-                    time_candidate(c);
-                }
+    for (uint32_t slack : slack_choices)
+        for (uint32_t pipe : pipe_choices)
+            for (uint32_t reg : reg_choices)
+                for (uint32_t w : warp_choices)
+                    for (uint32_t b : bit_choices) {
+                        Tuning c;
+                        c.warps = w;
+                        c.vh_bits = b;
+                        c.regs = reg;
+                        c.stage = stage_choices[0];
+                        c.pf = pf_choices[0];
+                        c.pipe = pipe;
+                        c.slack = slack;
+                        time_candidate(c);
+                    }
     // 1b. warps per query: the cooperative kernel (96 registers, vector
     // loads, one expansion at a time) at every table size.
     std::vector<uint32_t> wpq_choices = {2, 4};
@@ -1014,6 +1089,8 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
         return fail(ARTEA_GPU_EINVAL, "order_queries must be 0 (largest queue first) or ~0 (index order)");
     if (o.warps_per_query != 0 && o.warps_per_query != 1 && o.warps_per_query != 2 && o.warps_per_query != 4)
         return fail(ARTEA_GPU_EINVAL, "warps_per_query must be 0 (autotuned), 1, 2 or 4");
+    if (o.queue_slack != 0 && o.queue_slack != 0xffffffffu && o.queue_slack > 4096)
+        return fail(ARTEA_GPU_EINVAL, "queue_slack must be 0 (autotuned), 1..4096 (compact) or ~0 (2L)");
     DeviceGuard guard(ix->device);
     auto* r = new artea_gpu_router();
     r->idx = ix;
@@ -1034,6 +1111,7 @@ int artea_gpu_router_create(artea_gpu_index* ix, uint32_t topk, uint32_t queue, 
     r->want_prefetch = o.prefetch_rows;
     r->want_order = o.order_queries;
     r->want_wpq = o.warps_per_query;
+    r->want_slack = o.queue_slack;
     r->use_graphs = o.use_graphs != 0;
     r->words_per_slot = ((static_cast<uint64_t>(ix->n) + 127) / 128) * 4;   // multiple of 4 words
     r->list_cap = std::max<uint32_t>(std::min<uint32_t>(ix->n, 32768), 64);
@@ -1064,6 +1142,7 @@ int artea_gpu_router_destroy(artea_gpu_router* r) {
     dev_free(r->d_counter);
     dev_free(r->d_error);
     dev_free(r->d_order);
+    dev_free(r->d_overflow);
     dev_free(r->d_queries);
     dev_free(r->d_out);
     dev_free(r->d_topk);
@@ -1193,13 +1272,24 @@ int artea_gpu_router_tuning(const artea_gpu_router* r, uint32_t* warps_per_cta, 
 }
 
 int artea_gpu_router_tuning_ext(const artea_gpu_router* r, uint32_t* pipeline, uint32_t* prefetch_rows,
-                                uint32_t* ordered, uint32_t* warps_per_query) {
-    if (!r || !pipeline || !prefetch_rows || !ordered || !warps_per_query)
+                                uint32_t* ordered, uint32_t* warps_per_query, uint32_t* queue_slack) {
+    if (!r || !pipeline || !prefetch_rows || !ordered || !warps_per_query || !queue_slack)
         return fail(ARTEA_GPU_EINVAL, "null argument");
+    *queue_slack = r->last.slack;
     *pipeline = r->last_pipe ? 1u : 0u;
     *prefetch_rows = r->last.pf ? 16u : 8u;
     *ordered = r->last_ordered ? 1u : 0u;
     *warps_per_query = r->last.wpq;
+    return ARTEA_GPU_OK;
+}
+
+int artea_gpu_router_last_reruns(artea_gpu_router* r, uint32_t* reruns) {
+    if (!r || !reruns) return fail(ARTEA_GPU_EINVAL, "null argument");
+    *reruns = 0;
+    if (!r->d_overflow || !r->last.slack) return ARTEA_GPU_OK;
+    DeviceGuard guard(r->idx->device);
+    CUDA_TRY(cudaDeviceSynchronize());
+    CUDA_TRY(cudaMemcpy(reruns, r->d_overflow, sizeof(uint32_t), cudaMemcpyDeviceToHost));
     return ARTEA_GPU_OK;
 }
 

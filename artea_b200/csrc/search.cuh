@@ -89,6 +89,9 @@ struct SearchArgs {
     uint32_t coherent;        // queries/topk/queue may change while the kernel runs (serving ring)
     uint32_t early_stop;      // stop level-h greedy walks at distance <= es_thr[h]
     float es_thr[kMaxGroups]; // per-level thresholds in query distance units
+    uint32_t compact;         // queue capacity may be below 2L: a query that could lose a live
+                              // entry is abandoned and listed in overflow for the full-capacity rerun
+    uint32_t* __restrict__ overflow;   // [count, rerun counter, query indices...] (compact only)
     uint32_t l0_pipe;         // level-0 rows hold <= 64 distinct ids: pipelined level-0 loop
     uint32_t pf_l2;           // pipelined loop: also prefetch the second pass's rows into L2
     const uint32_t* __restrict__ order;   // persistent schedule: query order (null: 0..nq-1)
@@ -932,9 +935,14 @@ __device__ inline uint32_t queue_accept(const Queue& q, const uint32_t* cvid, co
 // in place (each lane holds at most two entries in registers). A vid word may
 // carry the explored bit (an entry popped before it is merged); ordering
 // ignores it.
-__device__ inline void queue_merge(Queue& q, float* bd, uint32_t* bv, uint32_t m) {
+// Returns true when an entry that may still be live was dropped: with a
+// capacity below 2L (the compact layout), entries past the capacity are not
+// kept; they are dead unless every kept entry past L ties lb, which is what
+// is reported (the caller then hands the query to the full-capacity rerun).
+__device__ inline bool queue_merge(Queue& q, float* bd, uint32_t* bv, uint32_t m) {
     const int lane = lane_id();
-    if (m == 0) return;
+    if (m == 0) return false;
+    const bool truncated = q.n + m > q.cap;
     {
         float sd[2];
         uint32_t sv[2], rk[2];
@@ -1014,13 +1022,14 @@ __device__ inline void queue_merge(Queue& q, float* bd, uint32_t* bv, uint32_t m
         }
         q.n = newn;
     }
+    return truncated && q.n == q.cap;
 }
 
 // try_push of a whole batch (bd/bv: scratch for the accepted entries).
-__device__ inline void queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, uint32_t cnt, float* bd, uint32_t* bv,
+__device__ inline bool queue_push_batch(Queue& q, uint32_t* cvid, float* cdist, uint32_t cnt, float* bd, uint32_t* bv,
                                         int* error) {
-    queue_merge(q, bd, bv, queue_accept(q, cvid, cdist, cnt, bd, bv));
     (void)error;
+    return queue_merge(q, bd, bv, queue_accept(q, cvid, cdist, cnt, bd, bv));
 }
 
 // The smallest accepted entry of bd/bv[0, m) by (dist, vid), m >= 1: its index
@@ -1104,9 +1113,15 @@ __host__ __device__ inline uint32_t stage_words(uint32_t dim, uint32_t stage_row
     return stage_rows ? 4u + stage_rows * (dim + kStagePad) : 0u;
 }
 
+// The queue's two arrays take an even number of entries each, so that the
+// regions after them (the 16-byte visited buckets, the next warp's area)
+// stay 16-byte aligned whatever the capacity (dim, the stage and the fixed
+// parts are multiples of 4 words).
+__host__ __device__ inline uint32_t queue_words(uint32_t cap) { return (cap + 1u) & ~1u; }
+
 __host__ __device__ inline uint32_t warp_smem_words(uint32_t dim, uint32_t cap, uint32_t vh_bits,
                                                     uint32_t stage_rows = 0) {
-    return dim + 2 * cap + 4 * kCandBatch + (vh_bits ? 4u * (1u << vh_bits) : 0u) + kPhaseWords +
+    return dim + 2 * queue_words(cap) + 4 * kCandBatch + (vh_bits ? 4u * (1u << vh_bits) : 0u) + kPhaseWords +
            stage_words(dim, stage_rows);
 }
 
@@ -1132,8 +1147,8 @@ __device__ __forceinline__ WarpSmem carve(float* base, uint32_t dim, uint32_t ca
     s.stage = stage_rows ? base + kPhaseWords + 4 : nullptr;
     s.q = base + kPhaseWords + stage_words(dim, stage_rows);
     s.qd = s.q + dim;
-    s.qv = reinterpret_cast<uint32_t*>(s.qd + cap);
-    s.cvid = s.qv + cap;
+    s.qv = reinterpret_cast<uint32_t*>(s.qd + queue_words(cap));
+    s.cvid = s.qv + queue_words(cap);
     s.cdist = reinterpret_cast<float*>(s.cvid + kCandBatch);
     s.bd = s.cdist + kCandBatch;
     s.bv = reinterpret_cast<uint32_t*>(s.bd + kCandBatch);
@@ -1164,8 +1179,9 @@ __device__ __forceinline__ WarpSmem carve(float* base, uint32_t dim, uint32_t ca
 // The chosen entry is marked explored where it lies: p2 in the array, a new
 // candidate in the batch before the merge places it.
 // ---------------------------------------------------------------------------
+// Returns true when the compact queue lost a live entry (see queue_merge).
 template <int kMetric, bool kExact, bool kRegs>
-__device__ __forceinline__ void l0_search_pipelined(const SearchArgs& a, Queue& q, Visited& vs, const WarpSmem& sm,
+__device__ __forceinline__ bool l0_search_pipelined(const SearchArgs& a, Queue& q, Visited& vs, const WarpSmem& sm,
                                                     float qsq, uint32_t cur, Counters& ct, PhaseClock& pc,
                                                     Stage& st) {
     const int lane = lane_id();
@@ -1255,9 +1271,10 @@ __device__ __forceinline__ void l0_search_pipelined(const SearchArgs& a, Queue& 
             pc.lap(kPhCollect);
         }
         // The current batch's merge runs while the next rows are loaded.
-        queue_merge(q, sm.bd, sm.bv, m);
+        const bool lost = queue_merge(q, sm.bd, sm.bv, m);
         __syncwarp();
         pc.lap(kPhMerge);
+        if (lost && a.compact) return true;
         if (!go) break;
         // Predict the entry after `next`: the first unexplored entry now.
         p2 = queue_find_unexplored(q, q.hint);
@@ -1272,6 +1289,7 @@ __device__ __forceinline__ void l0_search_pipelined(const SearchArgs& a, Queue& 
         pc.lap(kPhPop);
         cnt = ncnt;
     }
+    return false;
 }
 
 // ---------------------------------------------------------------------------
@@ -1295,7 +1313,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
     uint64_t* out = a.out + static_cast<size_t>(qi) * a.k_stride;
     constexpr uint64_t kInvalidWord = (static_cast<uint64_t>(0x7f7fffffu) << 32) | kVidMask;
 
-    if (topk > a.k_stride || L < topk || 2ull * L > a.cap) {
+    if (topk > a.k_stride || L < topk || (a.compact ? L + 1ull : 2ull * L) > a.cap) {
         set_error(a.error, kErrArgs);
         for (uint32_t i = lane; i < a.k_stride; i += 32) out[i] = kInvalidWord;
         return;
@@ -1303,6 +1321,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
 
     Counters ct = {};
     uint32_t nres = 0;
+    bool overflowed = false;
     PhaseClock pc;
     pc.start(a.phase_cycles != nullptr, sm.phase);
     const long long t_begin = pc.on ? clock64() : 0;
@@ -1406,7 +1425,8 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
         queue_insert(q, cur_d, cur, a.error);
         visited_set(vs, cur);
         if (kPipe && !kStage && kW == 1 && a.l0_pipe) {
-            l0_search_pipelined<kMetric, kExact, kRegs>(a, q, vs, sm, qsq, cur, ct, pc, st);
+            overflowed = l0_search_pipelined<kMetric, kExact, kRegs>(a, q, vs, sm, qsq, cur, ct, pc, st) &&
+                         a.compact;
         } else {
             // Software pipeline: while one row is processed, the row descriptor and
             // then the neighbour ids of the entry that would be expanded next are
@@ -1470,13 +1490,26 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                         pf_ids1 = lane + 32 < len2 ? __ldg(row2 + lane + 32) : 0xffffffffu;
                         pf_have_ids = true;
                     }
-                    queue_push_batch(q, cvid, cdist, cnt, sm.bd, sm.bv, a.error);
+                    overflowed = queue_push_batch(q, cvid, cdist, cnt, sm.bd, sm.bv, a.error) && a.compact;
                     __syncwarp();
                     pc.lap(kPhMerge);
+                    if (overflowed) break;
                 }
+                if (overflowed) break;
             }
         }
         visited_clear(vs);
+        if (overflowed) {
+            // The compact queue could have lost a live entry: the search is
+            // redone by the full-capacity rerun, which writes this row.
+            if (lane == 0) {
+                const uint32_t pos = atomicAdd(a.overflow, 1u);
+                a.overflow[2 + pos] = qi;
+            }
+            __syncwarp();
+            if (kStage) *stage_phase = st.phase;
+            return;
+        }
 
         // extract_results(min(topk, |T|)) (std_candidate_queue.hpp:542-561).
         const uint32_t tsize = min(q.n, q.L);
@@ -1563,6 +1596,23 @@ __global__ void __launch_bounds__(budget_threads(kBudget), budget_min_blocks(kBu
     if (kStage) {
         __syncwarp();
         if (lane_id() == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(sm.mbar)) : "memory");
+    }
+}
+
+// Full-capacity rerun of the queries a compact-queue launch abandoned
+// (a.overflow: count, work counter, indices). One warp per CTA, the queue at
+// 2L, the HBM bitset as visited set; CTAs with nothing to do exit at once.
+template <int kMetric, bool kExact>
+__global__ void __launch_bounds__(32, 24) search_rerun_kernel(SearchArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    const WarpSmem sm = carve(smem, a.g.dim, a.cap);
+    for (;;) {
+        uint32_t i = 0;
+        if (lane_id() == 0) i = atomicAdd(a.overflow + 1, 1u);
+        i = __shfl_sync(kFull, i, 0);
+        if (i >= __ldcg(a.overflow)) break;
+        const uint32_t qi = __ldcg(a.overflow + 2 + i);
+        search_one<kMetric, kExact>(a, qi, blockIdx.x, sm);
     }
 }
 

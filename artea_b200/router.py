@@ -205,7 +205,7 @@ class GpuRouter:
                  schedule: str = "auto", warps_per_cta: int = 0, ctas_per_sm: int = 0, max_batch: int = 0,
                  max_queue: int = 0, visited_hash_bits: int = 0, register_budget: int = 0,
                  use_graphs: bool = False, stage_rows: int = 0, pipeline: int = 0, prefetch_rows: int = 0,
-                 order_queries: int = 0, warps_per_query: int = 0):
+                 order_queries: int = 0, warps_per_query: int = 0, queue_slack: int = 0):
         opts = nat.RouterOpts()
         opts.metric = metric_code(metric)
         opts.mode = MODES[mode] if isinstance(mode, str) else int(mode)
@@ -221,6 +221,7 @@ class GpuRouter:
         opts.prefetch_rows = prefetch_rows
         opts.order_queries = order_queries
         opts.warps_per_query = warps_per_query
+        opts.queue_slack = queue_slack
         opts.use_graphs = 1 if use_graphs else 0
         h = ctypes.c_void_p()
         nat.check(nat.lib().artea_gpu_router_create(index.handle, topk, candidate_queue_size, ctypes.byref(opts),
@@ -296,12 +297,18 @@ class GpuRouter:
         w, b, g, st = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
         nat.check(nat.lib().artea_gpu_router_tuning(self._h, ctypes.byref(w), ctypes.byref(b), ctypes.byref(g),
                                                     ctypes.byref(st)))
-        p, pf, o, q = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        p, pf, o, q, sl = (ctypes.c_uint32() for _ in range(5))
         nat.check(nat.lib().artea_gpu_router_tuning_ext(self._h, ctypes.byref(p), ctypes.byref(pf), ctypes.byref(o),
-                                                        ctypes.byref(q)))
+                                                        ctypes.byref(q), ctypes.byref(sl)))
         return {"warps_per_cta": w.value, "visited_hash_bits": b.value, "register_budget": g.value,
                 "stage_rows": st.value, "pipeline": p.value, "prefetch_rows": pf.value, "ordered": o.value,
-                "warps_per_query": q.value}
+                "warps_per_query": q.value, "queue_slack": sl.value}
+
+    def last_reruns(self) -> int:
+        """Queries of the last compact-queue launch rerun at full capacity (waits)."""
+        n = ctypes.c_uint32()
+        nat.check(nat.lib().artea_gpu_router_last_reruns(self._h, ctypes.byref(n)))
+        return int(n.value)
 
     def launches(self) -> int:
         n = ctypes.c_uint64()

@@ -179,6 +179,14 @@ typedef struct artea_gpu_router_opts {
                                    split over the warps (for few, long
                                    searches: small batches, large dims);
                                    0 = autotuned */
+    uint32_t queue_slack;       /* persistent one-warp kernels' queue layout:
+                                   0xFFFFFFFF = 2L entries per search (room for
+                                   every tie of lb the reference keeps);
+                                   1..4096 = compact, max queue + that many
+                                   entries: a search that could lose a tie of
+                                   lb is abandoned and rerun at 2L by a second
+                                   kernel on the same stream, so results do
+                                   not change; 0 = autotuned (2L or +64) */
 } artea_gpu_router_opts;
 
 /* Library / device information. */
@@ -256,6 +264,11 @@ int artea_gpu_batch_query_l0_only(artea_gpu_router* router, const float* queries
 /* Waits for the router's stream and reports any kernel-side error. */
 int artea_gpu_router_sync(artea_gpu_router* router);
 
+/* Queries of this router's last compact-queue launch (queue_slack) that were
+ * handed to the full-capacity rerun; waits for the device. 0 for other
+ * layouts. No reference counterpart (measurement only). */
+int artea_gpu_router_last_reruns(artea_gpu_router* router, uint32_t* reruns);
+
 /* Number of kernel launches this router has issued (for launch accounting). */
 int artea_gpu_router_launches(const artea_gpu_router* router, uint64_t* launches);
 
@@ -318,10 +331,10 @@ int artea_gpu_router_tuning(const artea_gpu_router* router, uint32_t* warps_per_
                             uint32_t* register_budget, uint32_t* stage_rows);
 /* More of the last launch's parameters: pipelined level-0 loop (0/1),
  * neighbour rows loaded ahead (8 or 16), queries started largest queue first
- * (0/1), warps per query (1, 2, 4). No reference counterpart (measurement
- * only). */
+ * (0/1), warps per query (1, 2, 4), queue slack (0: 2L layout). No reference
+ * counterpart (measurement only). */
 int artea_gpu_router_tuning_ext(const artea_gpu_router* router, uint32_t* pipeline, uint32_t* prefetch_rows,
-                                uint32_t* ordered, uint32_t* warps_per_query);
+                                uint32_t* ordered, uint32_t* warps_per_query, uint32_t* queue_slack);
 
 /* ---- Serving loop (continuous batching) ----
  * No counterpart in the reference, whose batch_query is one blocking call; each

@@ -190,3 +190,49 @@ def test_autotuner_considers_warps_per_query(sift20k):
     assert r.tuning()["warps_per_query"] in (1, 2, 4)
     r.close()
     idx.close()
+
+
+# ---------------------------------------------------------------------------
+# Compact queue layout: max queue + slack entries per search instead of 2L; a
+# search that could lose a tie of lb is abandoned and rerun at 2L by a second
+# kernel. A slack of 1 or 2 on integer-valued data (many equal distances)
+# makes reruns frequent; words and counters must stay the reference's.
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", ["sift2k", "repeats", "axis80", "deep1k_cos"])
+@pytest.mark.parametrize("slack", [1, 2, 64])
+def test_compact_queue_matches_reference_fixtures(name, slack):
+    c = golden_case(name)
+    idx = DeviceIndex(c.graph, c.base)
+    reruns = 0
+    for L in c.queues:
+        for regs, pf in ((96, 8), (128, 16), (85, 8)):
+            r = GpuRouter(idx, c.metric, c.topk, L, mode="exact", schedule="persistent", warps_per_cta=2,
+                          visited_hash_bits=8, register_budget=regs, stage_rows=OFF, prefetch_rows=pf,
+                          queue_slack=slack)
+            out, st = r.batch_query(c.queries, stats=True)
+            np.testing.assert_array_equal(out, c.words[L], err_msg=f"{name} L={L} slack={slack} regs={regs}")
+            np.testing.assert_array_equal(st[:, 0].astype(np.uint64), c.calls[L])
+            assert r.tuning()["queue_slack"] == slack
+            reruns += r.last_reruns()
+            r.close()
+    if slack == 1 and name in ("sift2k", "repeats"):
+        assert reruns > 0, "a slack of 1 on tied distances should hand some searches to the rerun"
+    idx.close()
+
+
+@pytest.mark.parametrize("slack", [1, 64])
+def test_compact_queue_uneven_batch_matches_oracle(sift20k, uneven_ref, slack):
+    g, base, queries = sift20k
+    topk, queue, ref, ost = uneven_ref
+    idx = DeviceIndex(g, base)
+    for graphs in (False, True):
+        r = GpuRouter(idx, 0, 100, 512, mode="exact", schedule="persistent", warps_per_cta=4, visited_hash_bits=9,
+                      register_budget=96, stage_rows=OFF, prefetch_rows=8, queue_slack=slack, use_graphs=graphs)
+        for _ in range(2):
+            out, st = r.batch_query(queries, topk=topk, queue=queue, k_stride=100, stats=True)
+            np.testing.assert_array_equal(out, ref, err_msg=f"slack={slack} graphs={graphs}")
+            np.testing.assert_array_equal(st[:, :7], ost[:, :7])
+        if slack == 1:
+            assert r.last_reruns() > 0
+        r.close()
+    idx.close()
