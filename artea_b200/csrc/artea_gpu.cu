@@ -1318,7 +1318,11 @@ int artea_gpu_router_launches(const artea_gpu_router* r, uint64_t* launches) {
 //
 // Set-up: the first call on a device (with that device current) resolves the
 // array's device address with cudaGetSymbolAddress; make that first call
-// before any stream capture. All calls share the array and it keeps the last
+// before any stream capture. Under lazy module loading (the CUDA default
+// since 12.2) the array itself is placed when this library's module first
+// loads on the device (that first call, or the first launch of any kernel of
+// this library), so make that happen at start-up, before the caller reserves
+// its device memory. All calls share the array and it keeps the last
 // call's contents, so each call zeroes the part it uses before the launch;
 // calls that overlap on the GPU (for example on two streams) race on it and
 // must be serialised by the caller. The call waits for its kernel so that it

@@ -857,6 +857,8 @@ def main() -> None:
     ap.add_argument("--profile-pipeline", type=int, default=1, help="1: pipelined level-0 loop; 0: one expansion "
                                                                      "at a time")
     ap.add_argument("--profile-prefetch", type=int, default=8, help="rows loaded ahead: 8 or 16")
+    ap.add_argument("--profile-slack", type=int, default=0, help="compact queue slack (0: 2L layout)")
+    ap.add_argument("--profile-wpq", type=int, default=1, help="warps per query")
     ap.add_argument("--phases", action="store_true", help="with --profile: per-phase cycle breakdown")
     ap.add_argument("--uneven", action="store_true",
                     help="per-query topk in {10,100} and queue in {64,128,256,512} in one launch (the default for "
@@ -950,19 +952,28 @@ def main() -> None:
 
 
 def run_profile(args, w, queries, index, metric, device):
-    """One warm and one measured launch with fixed launch options (for ncu)."""
+    """One warm and one measured launch with fixed launch options (for ncu).
+    The deep workload (or --uneven) takes its per-query topk and queue."""
     import torch
     from artea_b200.router import GpuRouter
     nq, k = queries.shape[0], w.topk
     d_q = torch.from_numpy(queries).to(device)
+    d_tk = d_qu = None
+    L = args.profile_queue
+    if args.uneven or w.kind == "deep":
+        topk, queue = ds.per_query_params(w, nq)
+        k, L = int(topk.max()), int(queue.max())
+        d_tk = torch.from_numpy(topk.view(np.int32)).to(device)
+        d_qu = torch.from_numpy(queue.view(np.int32)).to(device)
     d_out = torch.empty((nq, k), dtype=torch.int64, device=device)
-    r = GpuRouter(index, metric, k, args.profile_queue, mode=args.mode,
+    r = GpuRouter(index, metric, k, L, mode=args.mode,
                   schedule="plain" if args.schedule == "plain" else "persistent",
                   warps_per_cta=args.profile_warps,
                   visited_hash_bits=args.profile_vh_bits if args.profile_vh_bits >= 0 else 0xFFFFFFFF,
                   register_budget=args.profile_regs, max_batch=nq,
                   stage_rows=args.profile_stage if args.profile_stage >= 0 else 0xFFFFFFFF,
-                  pipeline=0 if args.profile_pipeline else 0xFFFFFFFF, prefetch_rows=args.profile_prefetch)
+                  pipeline=1 if args.profile_pipeline else 0xFFFFFFFF, prefetch_rows=args.profile_prefetch,
+                  queue_slack=args.profile_slack or 0xFFFFFFFF, warps_per_query=args.profile_wpq)
     s = torch.cuda.current_stream(device)
     phases = torch.zeros((nq, 8), dtype=torch.int64, device=device) if args.phases else None
     for rep in range(2):
@@ -970,7 +981,7 @@ def run_profile(args, w, queries, index, metric, device):
             r.set_phase_buffer(phases)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        r.batch_query_device(d_q, nq, k, d_out, stream=s.cuda_stream)
+        r.batch_query_device(d_q, nq, k, d_out, d_topk=d_tk, d_queue=d_qu, stream=s.cuda_stream)
         e1.record(s)
         torch.cuda.synchronize(device)
         log(f"profile launch: {e0.elapsed_time(e1):.3f} ms for {nq} queries")

@@ -393,11 +393,18 @@ int artea_gpu_server_pause_heartbeat(artea_gpu_server* server);
  * nothing: its scratch memory is a fixed 64 MiB array that every GPU loading
  * this library holds until the process exits, so graphs whose per-CTA scratch
  * (4 warps x (N/8 + 16 KiB) bytes) exceeds 64 MiB, and queues above 1024, are
- * rejected with ARTEA_GPU_EINVAL. The first call on a device resolves the
- * array's address (make it before any stream capture); calls share the array,
- * so calls that overlap on the GPU race. Waits for its kernel before
- * returning. No counterpart in the reference, whose router always allocates
- * its visited tables and queues on the host. */
+ * rejected with ARTEA_GPU_EINVAL. The array exists once this library's module
+ * is loaded on the device; under CUDA's lazy module loading (the default since
+ * CUDA 12.2) that happens at the first call or the first launch of any of this
+ * library's kernels there, and it takes the array's 64 MiB then. So make one
+ * call (or one launch) per device at start-up, before device memory is
+ * reserved and before any stream capture; that first call also resolves the
+ * array's address. Calls share the array, so calls that overlap on the GPU
+ * race. The visited-id lists hold 4,096 ids per search (32,768 in the router),
+ * so large searches clear their bitsets whole more often: slower, same
+ * results. Waits for its kernel before returning. No counterpart in the
+ * reference, whose router always allocates its visited tables and queues on
+ * the host. */
 int artea_gpu_batch_query_noalloc(const artea_gpu_index* index, int metric, int mode, uint32_t topk,
                                   uint32_t queue_size, const float* d_queries, uint32_t nq, uint32_t k_stride,
                                   uint64_t* d_out, void* stream);

@@ -56,3 +56,26 @@ def test_noalloc_rejects_out_of_limit_arguments():
                                            None) == nat.EINVAL
     assert L.artea_gpu_batch_query_noalloc(idx.handle, 0, 0, 10, 32, None, 4, 10, nat.ptr(out), None) == nat.EINVAL
     idx.close()
+
+
+def test_noalloc_call_leaves_device_free_memory_unchanged():
+    # After a first call (which may load this library's module on the device,
+    # and with it the scratch array), a later call must not take any device
+    # memory: the free byte count the driver reports stays the same.
+    import torch
+    c = golden_case("sift2k")
+    idx = DeviceIndex(c.graph, c.base)
+    nq, k = c.queries.shape[0], c.topk
+    d_q = torch.from_numpy(np.ascontiguousarray(c.queries)).cuda()
+    out = torch.empty((nq, k), dtype=torch.int64, device=d_q.device)
+    L = nat.lib()
+    nat.check(L.artea_gpu_batch_query_noalloc(idx.handle, c.metric, 0, k, 32, nat.ptr(d_q), nq, k, nat.ptr(out), None))
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        nat.check(L.artea_gpu_batch_query_noalloc(idx.handle, c.metric, 0, k, 32, nat.ptr(d_q), nq, k, nat.ptr(out),
+                                                  None))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint64), c.words[32])
+    idx.close()
