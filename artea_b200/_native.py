@@ -87,6 +87,22 @@ class RouterOpts(ctypes.Structure):
     ]
 
 
+class ProbeResult(ctypes.Structure):
+    _fields_ = [
+        ("search_ms", ctypes.c_float),
+        ("greedy_ms", ctypes.c_float),
+        ("gather_ms", ctypes.c_float),
+        ("visited_ms", ctypes.c_float),
+        ("queue_ms", ctypes.c_float),
+        ("capped_queries", c_uint32),
+        ("candidates", c_uint64),
+        ("expansions", c_uint64),
+        ("gather_mismatches", c_uint32),
+        ("visited_mismatches", c_uint32),
+        ("queue_mismatches", c_uint32),
+    ]
+
+
 class ServerOpts(ctypes.Structure):
     _fields_ = [
         ("metric", c_int),
@@ -125,6 +141,8 @@ SIGNATURES = {
     "artea_gpu_router_sync": (c_int, [c_void_p]),
     "artea_gpu_router_launches": (c_int, [c_void_p, POINTER(c_uint64)]),
     "artea_gpu_router_last_reruns": (c_int, [c_void_p, POINTER(c_uint32)]),
+    "artea_gpu_subsystem_probe": (c_int, [c_void_p, c_int, c_int, c_uint32, c_uint32, c_void_p, c_uint32, c_uint32,
+                                          POINTER(ProbeResult)]),
     "artea_gpu_router_set_phase_buffer": (c_int, [c_void_p, c_void_p]),
     "artea_gpu_router_set_early_stop": (c_int, [c_void_p, c_void_p, c_uint32]),
     "artea_gpu_bruteforce": (c_int, [c_void_p, c_int, c_void_p, c_uint32, c_uint32, c_void_p, c_uint32, c_void_p]),

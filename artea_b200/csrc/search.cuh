@@ -64,6 +64,21 @@ struct DeviceGraph {
     const uint64_t* offsets[kMaxGroups];
 };
 
+// Trace of a search for the subsystem probes (kernels compiled with kTrace):
+// per query, the level-0 expansions (vid, new candidates), the candidates'
+// ids and distances in evaluation order, the cursor that seeds level 0, and
+// the lengths recorded (capped at cap / rows_cap).
+struct TraceArgs {
+    uint32_t* ids;       // nq x cap
+    float* dists;        // nq x cap
+    uint2* rows;         // nq x rows_cap: (expanded vid, new candidates)
+    uint2* cur;          // nq: (cursor vid, its distance bits)
+    uint2* len;          // nq: (candidates, rows) recorded
+    uint32_t cap;
+    uint32_t rows_cap;
+    uint32_t upper_only; // stop after the upper levels (the greedy descent alone)
+};
+
 struct SearchArgs {
     DeviceGraph g;
     const float* __restrict__ queries;
@@ -95,6 +110,7 @@ struct SearchArgs {
     uint32_t l0_pipe;         // level-0 rows hold <= 64 distinct ids: pipelined level-0 loop
     uint32_t pf_l2;           // pipelined loop: also prefetch the second pass's rows into L2
     const uint32_t* __restrict__ order;   // persistent schedule: query order (null: 0..nq-1)
+    TraceArgs tr;             // kernels compiled with kTrace only
 };
 
 // Phase-cycle breakdown written per query when phase_cycles is set.
@@ -1302,7 +1318,9 @@ __device__ __forceinline__ bool l0_search_pipelined(const SearchArgs& a, Queue& 
 // otherwise, and in kernels without it, one expansion at a time). kRegs: the
 // pipelined loop holds the next expansion's first pass in registers (the
 // 128-register budget) instead of prefetching it into L2. kW: warps per query.
-template <int kMetric, bool kExact, bool kStage = false, bool kRegs = false, int kW = 1, bool kPipe = false>
+// kTrace: record the search in a.tr (the probes' trace kernel).
+template <int kMetric, bool kExact, bool kStage = false, bool kRegs = false, int kW = 1, bool kPipe = false,
+          bool kTrace = false>
 __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, const WarpSmem& sm,
                            uint32_t* stage_phase = nullptr) {
     const int lane = lane_id();
@@ -1424,7 +1442,11 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
         q.lb = FLT_MAX;
         queue_insert(q, cur_d, cur, a.error);
         visited_set(vs, cur);
-        if (kPipe && !kStage && kW == 1 && a.l0_pipe) {
+        uint32_t tpos = 0, trows = 0;   // kTrace: candidates and rows recorded
+        if (kTrace && lane == 0) a.tr.cur[qi] = make_uint2(cur, __float_as_uint(cur_d));
+        if (kTrace && a.tr.upper_only) {
+            // The greedy descent alone: level 0 is not searched.
+        } else if (kPipe && !kStage && kW == 1 && a.l0_pipe) {
             overflowed = l0_search_pipelined<kMetric, kExact, kRegs>(a, q, vs, sm, qsq, cur, ct, pc, st) &&
                          a.compact;
         } else {
@@ -1477,9 +1499,23 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                     }
                     pos = consumed;
                     pc.lap(kPhCollect);
+                    if (kTrace) {
+                        if (lane == 0 && trows < a.tr.rows_cap)
+                            a.tr.rows[static_cast<size_t>(qi) * a.tr.rows_cap + trows] = make_uint2(v, cnt);
+                        ++trows;
+                    }
                     if (cnt == 0) continue;
                     dist_call<kMetric, kExact, kStage, kW>(g, sm.q, qsq, cvid, cdist, cnt, st, a.error, sm.coop);
                     ct.dist_evals += cnt;
+                    if (kTrace) {
+                        for (uint32_t i = lane; i < cnt; i += 32) {
+                            if (tpos + i < a.tr.cap) {
+                                a.tr.ids[static_cast<size_t>(qi) * a.tr.cap + tpos + i] = cvid[i];
+                                a.tr.dists[static_cast<size_t>(qi) * a.tr.cap + tpos + i] = cdist[i];
+                            }
+                        }
+                        tpos += cnt;
+                    }
                     pc.lap(kPhDist);
                     if (p2 >= 0 && !pf_have_ids) {
                         // The next entry's descriptor has arrived by now: fetch its ids
@@ -1498,6 +1534,8 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                 if (overflowed) break;
             }
         }
+        if (kTrace && lane == 0 && !a.tr.upper_only)
+            a.tr.len[qi] = make_uint2(min(tpos, a.tr.cap), min(trows, a.tr.rows_cap));
         visited_clear(vs);
         if (overflowed) {
             // The compact queue could have lost a live entry: the search is

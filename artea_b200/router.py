@@ -126,6 +126,16 @@ class DeviceIndex:
                                                  nat.ptr(sub), 0 if sub is None else sub.size, nat.ptr(out)))
         return out
 
+    def subsystem_probe(self, d_queries, nq: int, topk: int, queue: int, metric, mode: str = "exact",
+                        visited_hash_bits: int = 9) -> dict:
+        """The query path's subsystems run one at a time on a real search's
+        accesses (artea_gpu_subsystem_probe): per-probe milliseconds, work
+        recorded and the replays' mismatch counts (all 0 when faithful)."""
+        r = nat.ProbeResult()
+        nat.check(nat.lib().artea_gpu_subsystem_probe(self.handle, metric_code(metric), MODES[mode], topk, queue,
+                                                      nat.ptr(d_queries), nq, visited_hash_bits, ctypes.byref(r)))
+        return {name: getattr(r, name) for name, _ in nat.ProbeResult._fields_}
+
     def centroid_entry(self, metric, bucket: Optional[np.ndarray] = None) -> int:
         """The compactor's entry point: the bucket vid nearest to the bucket's
         centroid (artea_gpu_centroid_entry); 0xFFFFFFFF for an empty bucket."""

@@ -860,6 +860,9 @@ def main() -> None:
     ap.add_argument("--profile-slack", type=int, default=0, help="compact queue slack (0: 2L layout)")
     ap.add_argument("--profile-wpq", type=int, default=1, help="warps per query")
     ap.add_argument("--phases", action="store_true", help="with --profile: per-phase cycle breakdown")
+    ap.add_argument("--probe", action="store_true",
+                    help="subsystem probes at --profile-queue: the search traced, then the greedy descent, distance "
+                         "gathers, visited set and queue replayed alone (artea_gpu_subsystem_probe)")
     ap.add_argument("--uneven", action="store_true",
                     help="per-query topk in {10,100} and queue in {64,128,256,512} in one launch (the default for "
                          "the deep10m workload); compares the persistent and plain schedules")
@@ -913,6 +916,16 @@ def main() -> None:
     metric = metric_code(w.metric)
     if args.profile:
         run_profile(args, w, queries, index, metric, device)
+        index.close()
+        return
+    if args.probe:
+        import torch
+        d_q = torch.from_numpy(queries).to(device)
+        bits = args.profile_vh_bits if args.profile_vh_bits >= 0 else 0
+        res = index.subsystem_probe(d_q, queries.shape[0], w.topk, args.profile_queue, metric, mode=args.mode,
+                                    visited_hash_bits=bits)
+        print(json.dumps({"workload": w.name, "queue": args.profile_queue, "visited_hash_bits": bits, **res}),
+              flush=True)
         index.close()
         return
     if args.serve:

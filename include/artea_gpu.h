@@ -325,6 +325,36 @@ int artea_gpu_centroid_entry(const artea_gpu_index* index, int metric, const uin
  * turns it off. No reference counterpart (measurement only). */
 int artea_gpu_router_set_phase_buffer(artea_gpu_router* router, void* d_phase_cycles);
 
+/* Subsystem probes (measurement only; no reference counterpart). Runs the
+ * query path's subsystems one at a time on the memory accesses of a real
+ * search, so that each can be timed and profiled alone: a trace kernel
+ * (probe_trace_kernel) searches the nq device queries (EXACT or FAST, one
+ * topk and queue for all, visited table of 2^visited_hash_bits buckets, 0 =
+ * none) recording every level-0 expansion, its new candidates and their
+ * distances; then (a) the same kernel stops after the upper levels (the
+ * greedy descent alone), (d) probe_gather_kernel recomputes the recorded
+ * distances in the search's batches, (c) probe_visited_kernel reads every
+ * recorded expansion's row and passes it through the visited set, (b)
+ * probe_queue_kernel replays the recorded pops and pushes on the queue. Each
+ * replay checks itself against the trace (mismatches must be 0). The graph's
+ * level-0 rows must hold at most 64 distinct ids. Allocates its trace
+ * buffers (about nq * (4096 + 24 * queue) * 8 bytes) and waits. */
+typedef struct artea_gpu_probe_result {
+    float search_ms;          /* the trace kernel: the whole search */
+    float greedy_ms;          /* (a) upper levels only */
+    float gather_ms;          /* (d) distance gathers */
+    float visited_ms;         /* (c) visited set, with the row reads */
+    float queue_ms;           /* (b) queue pops and pushes */
+    uint32_t capped_queries;  /* queries whose trace hit its capacity */
+    uint64_t candidates;      /* level-0 distance evaluations recorded */
+    uint64_t expansions;      /* level-0 expansions recorded */
+    uint32_t gather_mismatches, visited_mismatches, queue_mismatches;
+} artea_gpu_probe_result;
+
+int artea_gpu_subsystem_probe(const artea_gpu_index* index, int metric, int mode, uint32_t topk,
+                              uint32_t queue_size, const float* d_queries, uint32_t nq,
+                              uint32_t visited_hash_bits, artea_gpu_probe_result* result);
+
 /* Launch parameters of the router's last launch (the autotuner's choice);
  * stage_rows 0 = vector loads, 8 = TMA-staged rows. */
 int artea_gpu_router_tuning(const artea_gpu_router* router, uint32_t* warps_per_cta, uint32_t* visited_hash_bits,

@@ -236,3 +236,36 @@ def test_compact_queue_uneven_batch_matches_oracle(sift20k, uneven_ref, slack):
             assert r.last_reruns() > 0
         r.close()
     idx.close()
+
+
+# ---------------------------------------------------------------------------
+# Subsystem probes: each replay of a recorded search must agree with the
+# trace (distances bit for bit, new-candidate counts, pop order), and the
+# trace must hold the search's level-0 work as the counters report it.
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name,L", [("sift2k", 32), ("sift2k", 100), ("deep1k_cos", 64), ("gist400", 50)])
+def test_subsystem_probes_replay_the_search(name, L):
+    import torch
+    c = golden_case(name)
+    idx = DeviceIndex(c.graph, c.base)
+    d_q = torch.from_numpy(np.ascontiguousarray(c.queries)).cuda()
+    res = idx.subsystem_probe(d_q, c.queries.shape[0], c.topk, L, c.metric, visited_hash_bits=8)
+    assert res["gather_mismatches"] == 0 and res["visited_mismatches"] == 0 and res["queue_mismatches"] == 0, res
+    assert res["capped_queries"] == 0
+    _, st = orc.batch_query(c.graph, c.base, c.queries, c.topk, L, metric=c.metric, stats=True)
+    st = st.astype(np.int64)
+    assert res["candidates"] == int((st[:, 0] - 1 - st[:, 5]).sum())
+    assert res["expansions"] == int(st[:, 3].sum())
+    assert min(res[k] for k in ("search_ms", "greedy_ms", "gather_ms", "visited_ms", "queue_ms")) > 0
+    idx.close()
+
+
+def test_subsystem_probe_rejects_rows_with_repeats():
+    import torch
+    from artea_b200 import _native as nat
+    c = golden_case("repeats")
+    idx = DeviceIndex(c.graph, c.base)
+    d_q = torch.from_numpy(np.ascontiguousarray(c.queries)).cuda()
+    with pytest.raises(nat.ArteaGpuError):
+        idx.subsystem_probe(d_q, c.queries.shape[0], c.topk, 32, c.metric)
+    idx.close()
