@@ -446,8 +446,11 @@ def max_over_ranks(dist, device, values):
 
 def our_launches(router, launches: int) -> int:
     """Kernels of ours per router launch: the search kernel, plus the query
-    order kernel when the persistent schedule ordered the batch."""
-    return launches * (2 if router.tuning().get("ordered") else 1)
+    order kernel when the persistent schedule ordered the batch, plus the
+    full-capacity rerun kernel under the compact queue layout (launched every
+    time; it exits at once when no search was handed to it)."""
+    t = router.tuning()
+    return launches * (1 + (1 if t.get("ordered") else 0) + (1 if t.get("queue_slack") else 0))
 
 
 def bench_uneven(args, w, base, queries, hgra, report, index, device, metric, cache_dir, rank, world, dist):
