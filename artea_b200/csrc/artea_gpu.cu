@@ -451,14 +451,9 @@ int prepare_launch(artea_gpu_router* r, SearchArgs a, bool persistent, const Tun
         a.overflow = r->d_overflow;
     }
     a.vh_bits = t.vh_bits;
-    {
-        uint32_t kb = 1;
-        while (kb < 32 && (1ull << kb) < r->idx->n) ++kb;
-        if (a.vh_bits && kb < a.vh_bits + 1) kb = a.vh_bits + 1;
-        a.vk_bits = kb;
-        // The 16-bit quotient (with 0xFFFF reserved) must hold kbits - tbits bits.
-        if (a.vh_bits && kb - a.vh_bits >= 16) return fail(ARTEA_GPU_EINVAL, "visited table too small for N");
-    }
+    // The 16-bit slot (0xFFFF reserved) must hold the quotient of kbits - tbits bits.
+    a.vk_bits = visited_kbits(r->idx->n, a.vh_bits);
+    if (!a.vk_bits) return fail(ARTEA_GPU_EINVAL, "visited table too small for N");
     p->fn = fn;
     p->persistent = persistent;
     if (coop) {
@@ -1396,11 +1391,12 @@ extern "C" int artea_gpu_batch_query_noalloc(const artea_gpu_index* ix, int metr
     // Launch shape: 4 warps per CTA, the 85-register kernel, an 8 KB
     // shared-memory visited table when the vid quotient fits in 15 bits.
     const uint32_t cap = std::max<uint32_t>(2u * queue_size, 2u);
-    uint32_t kb = 1;
-    while (kb < 32 && (1ull << kb) < ix->n) ++kb;
     uint32_t vh_bits = 9;
-    if (kb < vh_bits + 1) kb = vh_bits + 1;
-    if (kb - vh_bits >= 16) vh_bits = 0;
+    uint32_t kb = visited_kbits(ix->n, vh_bits);
+    if (!kb) {
+        vh_bits = 0;
+        kb = visited_kbits(ix->n, 0);
+    }
     const uint32_t smem = smem_bytes_per_warp(ix->dim, cap, vh_bits) * kNoAllocWarps;
     if (smem > 227u * 1024u) return fail(ARTEA_GPU_EINVAL, "no-alloc query: queue too large for shared memory");
     KernelFn fn = pick_kernel(metric, mode == ARTEA_GPU_MODE_EXACT, true, 0);

@@ -106,8 +106,8 @@ __global__ void __launch_bounds__(kProbeBudgetThreads, 5) probe_visited_kernel(S
     uint32_t* base = reinterpret_cast<uint32_t*>(smem) + static_cast<size_t>(warp) * (table_words + kCandBatch);
     uint32_t* cvid = base + table_words;
     Visited vs;
-    vs.tab = reinterpret_cast<uint4*>(base);
-    vs.tbits = a.vh_bits;
+    vs.tab = reinterpret_cast<uint2*>(base);
+    vs.tbits = a.vh_bits ? a.vh_bits + 1 : 0u;
     vs.kbits = a.vk_bits;
     vs.kmask = a.vk_bits >= 32 ? 0xFFFFFFFFu : ((1u << a.vk_bits) - 1u);
     vs.bits = a.vis_bits + static_cast<size_t>(slot) * a.words_per_slot;
@@ -307,11 +307,8 @@ extern "C" int artea_gpu_subsystem_probe(const artea_gpu_index* ix, int metric, 
     a.k_stride = topk;
     a.cap = std::max<uint32_t>(2u * queue_size, 2u);
     a.vh_bits = visited_hash_bits;
-    uint32_t kb = 1;
-    while (kb < 32 && (1ull << kb) < ix->n) ++kb;
-    if (a.vh_bits && kb < a.vh_bits + 1) kb = a.vh_bits + 1;
-    if (a.vh_bits && kb - a.vh_bits >= 16) return fail(ARTEA_GPU_EINVAL, "probe: visited table too small for N");
-    a.vk_bits = kb;
+    a.vk_bits = visited_kbits(ix->n, a.vh_bits);
+    if (!a.vk_bits) return fail(ARTEA_GPU_EINVAL, "probe: visited table too small for N");
     a.words_per_slot = ((static_cast<uint64_t>(ix->n) + 127) / 128) * 4;
     a.list_cap = std::max<uint32_t>(std::min<uint32_t>(ix->n, 32768), 64);
 

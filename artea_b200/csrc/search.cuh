@@ -89,8 +89,8 @@ struct SearchArgs {
     uint32_t queue_default;
     uint32_t k_stride;
     uint32_t cap;                         // queue entries per warp (>= 2 * max queue)
-    uint32_t vh_bits;                     // log2 of the shared-memory visited bucket count (0: none)
-    uint32_t vk_bits;                     // log2 of the vid permutation space (>= log2 N, > vh_bits)
+    uint32_t vh_bits;                     // log2 of the shared-memory visited table in 16-byte units (0: none)
+    uint32_t vk_bits;                     // log2 of the vid permutation space (visited_kbits)
     uint64_t* __restrict__ out;
     artea_gpu_query_stats* __restrict__ stats;   // may be null
     uint32_t* __restrict__ vis_bits;      // slots x words_per_slot
@@ -461,24 +461,41 @@ __device__ void coop_helper(const DeviceGraph& g, const float* __restrict__ q, C
 // ---------------------------------------------------------------------------
 // Visited set (subsystem c): exact, in two tiers.
 //   1. A bucketed table in shared memory. vid -> p = (vid * odd) mod 2^kbits is
-//      a bijection, so (bucket = high tbits bits of p, quotient = the other
-//      kbits - tbits bits) identifies vid exactly; a bucket is 8 uint16
-//      quotients (16 bytes), read with one vector load. 0xFFFF marks an
-//      empty slot (quotients have at most 15 bits).
+//      a bijection, so (bucket A = high tbits bits of p, quotient Q = the other
+//      kbits - tbits bits) identifies vid exactly; a bucket is 4 uint16 slots
+//      (8 bytes, one load), 0xFFFF marks an empty slot. When the quotient has
+//      at most 14 bits, an id whose bucket A is full goes to a second bucket
+//      B = A ^ alt(Q), stored as Q | 0x8000: the flag keeps it apart from
+//      B's own ids (whose slots hold flag-free quotients), and B with Q gives
+//      back A and so the id. Buckets only fill up, never drain, until clear():
+//      an id absent from A while A has a free slot was never visited (it would
+//      only have gone to B with A full), likewise for B.
 //   2. The slot's bitset in HBM (atomicOr = test_and_set,
-//      containers/version_tag_table.hpp:128-132), used for ids whose bucket is
-//      full. Buckets only fill up, never drain, until clear(): an id absent
-//      from a bucket that still has a free slot was never visited; only ids
-//      hashing to a full bucket need the bitset.
+//      containers/version_tag_table.hpp:128-132), used for ids whose buckets
+//      are full.
 // Ids set in the bitset are listed so clear() (a version bump in the
 // reference, version_tag_table.hpp:142-148) zeroes only the words it touched,
 // or the whole bitset if the list overflowed. With no table (tbits == 0)
 // every id goes to the bitset.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kVisitedMul = 0x9E3779B1u;   // odd: multiplication mod 2^k is a bijection
+constexpr uint32_t kAltFlag = 0x8000u;          // slot holds an id whose first bucket was full
+
+// Permutation space of the table for a graph of n vertices and a table of
+// 16 << table_log bytes (2^(table_log + 1) buckets of 8 bytes): returns kbits
+// (>= log2 n and > the bucket bits), or 0 when a quotient would not fit in
+// 15 bits (table too small for n).
+__host__ __device__ inline uint32_t visited_kbits(uint32_t n, uint32_t table_log) {
+    uint32_t kb = 1;
+    while (kb < 32 && (1ull << kb) < n) ++kb;
+    if (table_log == 0) return kb;
+    const uint32_t tbits = table_log + 1;
+    if (kb < tbits + 1) kb = tbits + 1;
+    return kb - tbits > 15 ? 0u : kb;
+}
 
 struct Visited {
-    uint4* tab;         // shared-memory buckets
+    uint2* tab;         // shared-memory buckets (4 uint16 slots each)
     uint32_t tbits;     // log2 of the bucket count (0: no table)
     uint32_t kbits;     // log2 of the permutation space
     uint32_t kmask;     // 2^kbits - 1
@@ -492,30 +509,60 @@ struct Visited {
     uint32_t spills;
 };
 
-// Returns 1 if vid is in its bucket, 0 if it was inserted now, 2 if its
-// bucket is full (the bitset decides).
-__device__ __forceinline__ int table_test_insert(const Visited& vs, uint32_t vid) {
+// One id's walk through the table: the bucket to read, the slot value looked
+// for (and inserted), and the second bucket while it is still to come.
+struct TableWalk {
+    uint32_t bucket;
+    uint32_t val;
+    uint32_t alt;       // the second bucket, or ~0u when there is none
+};
+
+__device__ __forceinline__ TableWalk table_walk(const Visited& vs, uint32_t vid) {
     const uint32_t p = (vid * kVisitedMul) & vs.kmask;
     const uint32_t qbits = vs.kbits - vs.tbits;
-    const uint32_t bucket = p >> qbits;
-    const uint32_t quot = p & ((1u << qbits) - 1u);   // < 0x8000 by construction
-    const uint32_t pair = quot | (quot << 16);
-    uint32_t* w = reinterpret_cast<uint32_t*>(vs.tab + bucket);
-    for (int attempt = 0; attempt < 16; ++attempt) {
-        const uint4 b = vs.tab[bucket];
-        if (__vcmpeq2(b.x, pair) | __vcmpeq2(b.y, pair) | __vcmpeq2(b.z, pair) | __vcmpeq2(b.w, pair)) return 1;
-        const uint32_t e0 = __vcmpeq2(b.x, 0xFFFFFFFFu), e1 = __vcmpeq2(b.y, 0xFFFFFFFFu);
-        const uint32_t e2 = __vcmpeq2(b.z, 0xFFFFFFFFu), e3 = __vcmpeq2(b.w, 0xFFFFFFFFu);
-        int wi;
-        uint32_t old, e;
-        if (e0) { wi = 0; old = b.x; e = e0; }
-        else if (e1) { wi = 1; old = b.y; e = e1; }
-        else if (e2) { wi = 2; old = b.z; e = e2; }
-        else if (e3) { wi = 3; old = b.w; e = e3; }
-        else return 2;
-        const uint32_t desired = (e & 0xFFFFu) ? ((old & 0xFFFF0000u) | quot) : ((old & 0x0000FFFFu) | (quot << 16));
-        if (atomicCAS(w + wi, old, desired) == old) return 0;
-        // Another lane filled that slot meanwhile: read the bucket again.
+    TableWalk w;
+    w.bucket = p >> qbits;
+    const uint32_t q = p & ((1u << qbits) - 1u);
+    w.val = q;
+    // alt(Q): the second bucket's offset from the quotient's bits (0 would
+    // give B == A: no second choice for that quotient).
+    const uint32_t h = (q * 0x2545F491u) >> (32u - vs.tbits);
+    w.alt = (qbits <= 14 && h != 0) ? (w.bucket ^ h) : 0xffffffffu;
+    return w;
+}
+
+// One bucket read (and at most one CAS) of a walk: -1 while the walk goes on,
+// else 1 (the id is present), 0 (inserted now) or 2 (its buckets are full:
+// the bitset decides).
+__device__ __forceinline__ int table_step(const Visited& vs, TableWalk& w) {
+    const uint2 b = vs.tab[w.bucket];
+    const uint32_t pair = w.val | (w.val << 16);
+    if (__vcmpeq2(b.x, pair) | __vcmpeq2(b.y, pair)) return 1;
+    const uint32_t e0 = __vcmpeq2(b.x, 0xFFFFFFFFu), e1 = __vcmpeq2(b.y, 0xFFFFFFFFu);
+    if (!(e0 | e1)) {
+        if (w.alt == 0xffffffffu) return 2;
+        // The first bucket is full: the second decides.
+        w.bucket = w.alt;
+        w.val |= kAltFlag;
+        w.alt = 0xffffffffu;
+        return -1;
+    }
+    const int wi = e0 ? 0 : 1;
+    const uint32_t old = e0 ? b.x : b.y;
+    const uint32_t e = e0 ? e0 : e1;
+    const uint32_t desired = (e & 0xFFFFu) ? ((old & 0xFFFF0000u) | w.val) : ((old & 0x0000FFFFu) | (w.val << 16));
+    uint32_t* word = reinterpret_cast<uint32_t*>(vs.tab + w.bucket) + wi;
+    if (atomicCAS(word, old, desired) == old) return 0;
+    return -1;   // another lane filled that slot meanwhile: read the bucket again
+}
+
+// Returns 1 if vid is in the table, 0 if it was inserted now, 2 if its
+// buckets are full (the bitset decides).
+__device__ __forceinline__ int table_test_insert(const Visited& vs, uint32_t vid) {
+    TableWalk w = table_walk(vs, vid);
+    for (int step = 0; step < 24; ++step) {
+        const int r = table_step(vs, w);
+        if (r >= 0) return r;
     }
     return 2;
 }
@@ -555,66 +602,18 @@ __device__ __forceinline__ void visited_set(Visited& vs, uint32_t vid) {
     visited_test_and_set(vs, vid, lane_id() == 0);
 }
 
-// table_test_insert for two distinct ids per lane, the two dependency chains
+// table_test_insert for two distinct ids per lane, the two walks
 // interleaved. r0/r1 as table_test_insert's return values (-1: inactive).
 __device__ __forceinline__ void table_test_insert2(const Visited& vs, uint32_t v0, bool a0, uint32_t v1, bool a1,
                                                    int* r0, int* r1) {
-    const uint32_t qbits = vs.kbits - vs.tbits;
-    const uint32_t qmask = (1u << qbits) - 1u;
-    const uint32_t p0 = (v0 * kVisitedMul) & vs.kmask, p1 = (v1 * kVisitedMul) & vs.kmask;
-    const uint32_t bk0 = p0 >> qbits, bk1 = p1 >> qbits;
-    const uint32_t q0 = p0 & qmask, q1 = p1 & qmask;
-    const uint32_t pair0 = q0 | (q0 << 16), pair1 = q1 | (q1 << 16);
-    bool pend0 = a0, pend1 = a1;
-    *r0 = a0 ? 2 : -1;
-    *r1 = a1 ? 2 : -1;
-    for (int attempt = 0; attempt < 16 && (pend0 || pend1); ++attempt) {
-        const uint4 b0 = vs.tab[pend0 ? bk0 : 0];
-        const uint4 b1 = vs.tab[pend1 ? bk1 : 0];
-        int wi0 = -1, wi1 = -1;
-        uint32_t old0 = 0, old1 = 0, des0 = 0, des1 = 0;
-        if (pend0) {
-            if (__vcmpeq2(b0.x, pair0) | __vcmpeq2(b0.y, pair0) | __vcmpeq2(b0.z, pair0) | __vcmpeq2(b0.w, pair0)) {
-                *r0 = 1;
-                pend0 = false;
-            } else {
-                const uint32_t e0 = __vcmpeq2(b0.x, 0xFFFFFFFFu), e1 = __vcmpeq2(b0.y, 0xFFFFFFFFu);
-                const uint32_t e2 = __vcmpeq2(b0.z, 0xFFFFFFFFu), e3 = __vcmpeq2(b0.w, 0xFFFFFFFFu);
-                uint32_t e;
-                if (e0) { wi0 = 0; old0 = b0.x; e = e0; }
-                else if (e1) { wi0 = 1; old0 = b0.y; e = e1; }
-                else if (e2) { wi0 = 2; old0 = b0.z; e = e2; }
-                else if (e3) { wi0 = 3; old0 = b0.w; e = e3; }
-                else { e = 0; pend0 = false; }   // full: the bitset decides (r0 stays 2)
-                if (pend0) des0 = (e & 0xFFFFu) ? ((old0 & 0xFFFF0000u) | q0) : ((old0 & 0x0000FFFFu) | (q0 << 16));
-            }
-        }
-        if (pend1) {
-            if (__vcmpeq2(b1.x, pair1) | __vcmpeq2(b1.y, pair1) | __vcmpeq2(b1.z, pair1) | __vcmpeq2(b1.w, pair1)) {
-                *r1 = 1;
-                pend1 = false;
-            } else {
-                const uint32_t e0 = __vcmpeq2(b1.x, 0xFFFFFFFFu), e1 = __vcmpeq2(b1.y, 0xFFFFFFFFu);
-                const uint32_t e2 = __vcmpeq2(b1.z, 0xFFFFFFFFu), e3 = __vcmpeq2(b1.w, 0xFFFFFFFFu);
-                uint32_t e;
-                if (e0) { wi1 = 0; old1 = b1.x; e = e0; }
-                else if (e1) { wi1 = 1; old1 = b1.y; e = e1; }
-                else if (e2) { wi1 = 2; old1 = b1.z; e = e2; }
-                else if (e3) { wi1 = 3; old1 = b1.w; e = e3; }
-                else { e = 0; pend1 = false; }
-                if (pend1) des1 = (e & 0xFFFFu) ? ((old1 & 0xFFFF0000u) | q1) : ((old1 & 0x0000FFFFu) | (q1 << 16));
-            }
-        }
-        // A failed CAS means another insert filled that slot: read the bucket again.
-        if (pend0 && atomicCAS(reinterpret_cast<uint32_t*>(vs.tab + bk0) + wi0, old0, des0) == old0) {
-            *r0 = 0;
-            pend0 = false;
-        }
-        if (pend1 && atomicCAS(reinterpret_cast<uint32_t*>(vs.tab + bk1) + wi1, old1, des1) == old1) {
-            *r1 = 0;
-            pend1 = false;
-        }
+    TableWalk w0 = table_walk(vs, a0 ? v0 : 0u), w1 = table_walk(vs, a1 ? v1 : 0u);
+    int t0 = a0 ? -1 : -2, t1 = a1 ? -1 : -2;
+    for (int step = 0; step < 24 && (t0 == -1 || t1 == -1); ++step) {
+        if (t0 == -1) t0 = table_step(vs, w0);
+        if (t1 == -1) t1 = table_step(vs, w1);
     }
+    *r0 = a0 ? (t0 < 0 ? 2 : t0) : -1;
+    *r1 = a1 ? (t1 < 0 ? 2 : t1) : -1;
 }
 
 // test_and_set for two ids per lane; all the ids of the warp are distinct.
@@ -654,8 +653,10 @@ __device__ __forceinline__ void visited_test_and_set2(Visited& vs, uint32_t v0, 
 
 __device__ __forceinline__ void table_reset(const Visited& vs) {
     if (vs.tbits) {
-        const uint32_t n = 1u << vs.tbits;
-        for (uint32_t i = lane_id(); i < n; i += 32) vs.tab[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
+        // Two buckets per 16-byte store.
+        uint4* t4 = reinterpret_cast<uint4*>(vs.tab);
+        const uint32_t n = 1u << (vs.tbits - 1);
+        for (uint32_t i = lane_id(); i < n; i += 32) t4[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
     }
 }
 
@@ -1344,8 +1345,8 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
     pc.start(a.phase_cycles != nullptr, sm.phase);
     const long long t_begin = pc.on ? clock64() : 0;
     Visited vs;
-    vs.tab = reinterpret_cast<uint4*>(sm.vh);
-    vs.tbits = a.vh_bits;
+    vs.tab = reinterpret_cast<uint2*>(sm.vh);
+    vs.tbits = a.vh_bits ? a.vh_bits + 1 : 0u;   // a.vh_bits: log2 of the table's 16-byte units
     vs.kbits = a.vk_bits;
     vs.kmask = a.vk_bits >= 32 ? 0xFFFFFFFFu : ((1u << a.vk_bits) - 1u);
     vs.bits = a.vis_bits + static_cast<size_t>(slot) * a.words_per_slot;

@@ -338,12 +338,12 @@ extern "C" int artea_gpu_server_create(artea_gpu_index* ix, const artea_gpu_serv
     s->idle_limit = 0xFFFFFFFFu;
     s->beat_limit_ms = o.heartbeat_ms ? o.heartbeat_ms : 2000u;
     s->cap = std::max<uint32_t>(2u * s->qmax, 2u);
-    uint32_t kb = 1;
-    while (kb < 32 && (1ull << kb) < ix->n) ++kb;
     s->vh_bits = 8;
-    if (kb < s->vh_bits + 1) kb = s->vh_bits + 1;
-    if (kb - s->vh_bits >= 16) s->vh_bits = 0;
-    s->vk_bits = kb;
+    s->vk_bits = visited_kbits(ix->n, s->vh_bits);
+    if (!s->vk_bits) {
+        s->vh_bits = 0;
+        s->vk_bits = visited_kbits(ix->n, 0);
+    }
     s->fn = pick_serve(o.metric, o.mode == ARTEA_GPU_MODE_EXACT);
     s->smem = warp_smem_words(ix->dim, s->cap, s->vh_bits) * 4u * s->warps;
     if (s->smem > 227u * 1024u) return cleanup(fail(ARTEA_GPU_EINVAL, "max_queue too large for shared memory"));

@@ -141,9 +141,10 @@ typedef struct artea_gpu_router_opts {
     uint32_t max_batch;      /* largest nq one call may pass; 0 = 65536 */
     uint32_t max_queue;      /* largest per-query queue size; 0 = candidate_queue_size */
     uint32_t use_graphs;     /* capture launches in CUDA graphs and replay them */
-    uint32_t visited_hash_bits; /* log2 of the bucket count of the per-warp
-                                   shared-memory visited table (16 bytes per
-                                   bucket), in [6, 12]; 0 = autotuned;
+    uint32_t visited_hash_bits; /* log2 of the size of the per-warp
+                                   shared-memory visited table in 16-byte
+                                   units (8 ids per unit, two buckets of 4),
+                                   in [6, 12]; 0 = autotuned;
                                    0xFFFFFFFF = no table (HBM bitset only) */
     uint32_t register_budget;   /* registers per thread of the persistent kernel:
                                    64 (32 warps per SM), 85 (80 used, 24
@@ -329,7 +330,7 @@ int artea_gpu_router_set_phase_buffer(artea_gpu_router* router, void* d_phase_cy
  * query path's subsystems one at a time on the memory accesses of a real
  * search, so that each can be timed and profiled alone: a trace kernel
  * (probe_trace_kernel) searches the nq device queries (EXACT or FAST, one
- * topk and queue for all, visited table of 2^visited_hash_bits buckets, 0 =
+ * topk and queue for all, visited table of 16 << visited_hash_bits bytes, 0 =
  * none) recording every level-0 expansion, its new candidates and their
  * distances; then (a) the same kernel stops after the upper levels (the
  * greedy descent alone), (d) probe_gather_kernel recomputes the recorded
