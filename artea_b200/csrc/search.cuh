@@ -947,6 +947,16 @@ __device__ inline uint32_t queue_accept(const Queue& q, const uint32_t* cvid, co
     return m;
 }
 
+// Number of entries of the sorted array q[0, n) before (d, v) by (dist, vid).
+__device__ __forceinline__ uint32_t old_lower_bound(const Queue& q, float d, uint32_t v) {
+    uint32_t lo = 0, hi = q.n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (entry_less(q.d[mid], q.v[mid], d, v)) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
 // Merges the m (<= kCandBatch) accepted entries of bd/bv into the sorted
 // array and trims it at the new lb. The batch is first sorted by (dist, vid)
 // in place (each lane holds at most two entries in registers). A vid word may
@@ -985,49 +995,52 @@ __device__ inline bool queue_merge(Queue& q, float* bd, uint32_t* bv, uint32_t m
         }
         __syncwarp();
     }
-    // Final positions of the batch entries: rank in the old array + rank in the batch.
-    uint32_t posb[2] = {0xffffffffu, 0xffffffffu};
-    for (uint32_t r = lane, t = 0; r < m; r += 32, ++t) {
-        const float d = bd[r];
-        const uint32_t v = bv[r];
-        uint32_t lo = 0, hi = q.n;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (entry_less(q.d[mid], q.v[mid], d, v)) lo = mid + 1; else hi = mid;
+    // Final positions of the batch entries: rank in the old array + rank in
+    // the batch (sorted, distinct); lanes past m hold a sentinel above every
+    // position.
+    constexpr int kNoPos = 0x7fffffff;
+    int posb0 = kNoPos, posb1 = kNoPos;
+    if (static_cast<uint32_t>(lane) < m) posb0 = static_cast<int>(old_lower_bound(q, bd[lane], bv[lane]) + lane);
+    const bool two = m > 32u;
+    if (two && static_cast<uint32_t>(lane) + 32u < m)
+        posb1 = static_cast<int>(old_lower_bound(q, bd[lane + 32], bv[lane + 32]) + lane + 32u);
+    const int p0 = __shfl_sync(kFull, posb0, 0);   // position of the smallest batch entry
+    // Output positions [p0, end) change. Output o holds batch entry r when
+    // o = posb_r, else the old entry o - #{r : posb_r < o}, which lies at or
+    // before o; within a chunk of 32 outputs every lane reads its source
+    // before any lane writes. Chunks go tail first: a chunk's sources lie
+    // before the outputs of every chunk written earlier.
+    const int end = static_cast<int>(min(q.n + m, q.cap));
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int cb = end - 32; cb + 32 > p0; cb -= 32) {
+        const uint32_t rel0 = static_cast<uint32_t>(posb0) - static_cast<uint32_t>(cb);
+        const uint32_t rel1 = static_cast<uint32_t>(posb1) - static_cast<uint32_t>(cb);
+        uint32_t mask = __reduce_or_sync(kFull, rel0 < 32u ? 1u << rel0 : 0u);   // batch outputs in the chunk
+        uint32_t nb = __popc(__ballot_sync(kFull, posb0 < cb));                 // batch outputs before it
+        if (two) {
+            mask |= __reduce_or_sync(kFull, rel1 < 32u ? 1u << rel1 : 0u);
+            nb += __popc(__ballot_sync(kFull, posb1 < cb));
         }
-        posb[t] = lo + r;
-    }
-    const uint32_t p0 = __shfl_sync(kFull, posb[0], 0);   // position of the smallest batch entry
-    // Move the old entries from p0 on to the right by the number of batch
-    // entries smaller than them, tail first (targets never overlap unread ones).
-    for (int end = static_cast<int>(q.n); end > static_cast<int>(p0); end -= 32) {
-        const int s0 = max(static_cast<int>(p0), end - 32);
-        const int i = s0 + lane;
-        const bool act = i < end;
+        const int before = static_cast<int>(nb + __popc(mask & lt));
+        const int o = cb + lane;
+        const bool act = o >= p0;
+        const bool from_batch = (mask >> lane) & 1u;
         float dd = 0.f;
-        uint32_t vv = 0;
-        uint32_t np = 0xffffffffu;
+        uint32_t vv = 0u;
         if (act) {
-            dd = q.d[i];
-            vv = q.v[i];
-            uint32_t lo = 0, hi = m;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (entry_less(bd[mid], bv[mid], dd, vv)) lo = mid + 1; else hi = mid;
-            }
-            np = static_cast<uint32_t>(i) + lo;
+            dd = from_batch ? bd[before] : q.d[o - before];
+            vv = from_batch ? bv[before] : q.v[o - before];
         }
         __syncwarp();
-        if (act && np < q.cap) { q.d[np] = dd; q.v[np] = vv; }
-        __syncwarp();
-    }
-    for (uint32_t r = lane, t = 0; r < m; r += 32, ++t) {
-        if (posb[t] < q.cap) { q.d[posb[t]] = bd[r]; q.v[posb[t]] = bv[r]; }
+        if (act) {
+            q.d[o] = dd;
+            q.v[o] = vv;
+        }
     }
     __syncwarp();
     const uint32_t total = min(q.n + m, q.cap);
     q.n = total;
-    if (p0 < q.hint) q.hint = p0;
+    if (static_cast<uint32_t>(p0) < q.hint) q.hint = static_cast<uint32_t>(p0);
     if (q.n >= q.L) {
         q.lb = q.d[q.L - 1];
         uint32_t newn = q.n;

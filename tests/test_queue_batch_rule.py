@@ -140,3 +140,47 @@ def test_rule_counts_earlier_candidates_of_the_same_row():
         q.push_row([(1.0, 3), (1.0, 4), (1.0, 5), (0.5, 6)])
     assert sorted(seq.T) == bat.top() == [(0.5, 6), (1.0, 3)]
     assert seq.expandable() == bat.expandable()
+
+
+def gather_merge(old, batch, cap):
+    """queue_merge's move step as the kernel runs it: final batch positions
+    (rank in the old array + rank in the batch), then output chunks of 32,
+    tail first, each lane reading its source (batch entry, or old entry
+    o - #{batch positions < o}) before any lane of the chunk writes, in place."""
+    n, m = len(old), len(batch)
+    a = list(old) + [None] * (cap - n)
+    batch = sorted(batch)
+    posb = [sum(1 for e in old if e < b) + r for r, b in enumerate(batch)]
+    p0, end = posb[0], min(n + m, cap)
+    cb = end - 32
+    while cb + 32 > p0:
+        mask = 0
+        for p in posb:
+            if 0 <= p - cb < 32:
+                mask |= 1 << (p - cb)
+        nb = sum(1 for p in posb if p < cb)
+        reads = []
+        for lane in range(32):
+            o = cb + lane
+            if o < p0:
+                continue
+            before = nb + bin(mask & ((1 << lane) - 1)).count("1")
+            reads.append((o, batch[before] if (mask >> lane) & 1 else a[o - before]))
+        for o, e in reads:
+            a[o] = e
+        cb -= 32
+    return a[:end]
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_gather_merge_moves_equal_a_sorted_merge(seed):
+    # The in-place chunked moves give the sorted union cut at the capacity,
+    # for batches of 1..64 entries landing anywhere, with and without truncation.
+    rng = np.random.default_rng(2000 + seed)
+    for _ in range(400):
+        n = int(rng.integers(0, 700))
+        m = int(rng.integers(1, 65))
+        cap = n + int(rng.integers(0, 80)) if rng.random() < 0.5 else 1100
+        keys = [(float(d), int(v)) for d, v in zip(rng.integers(0, 40, n + m), rng.permutation(100000)[: n + m])]
+        old, batch = sorted(keys[:n]), keys[n:]
+        assert gather_merge(old, batch, cap) == sorted(keys)[: min(n + m, cap)]
