@@ -121,6 +121,35 @@ struct artea_gpu_router {
 
 namespace artea_gpu {
 
+// x.x of every vector row, accumulated as the cosine distance accumulates it
+// (4 lanes per row, lane group g owning elements 16c + 4g .. 16c + 4g + 3 of
+// every chunk c, one FMA chain per element position, then the 16-lane fold
+// of the exact mode), so the stored value equals the one the distance kernel
+// would compute for the row (utils/simd_distance.hpp:251-274, x's norm).
+__global__ void row_sqnorm_kernel(const float* __restrict__ vecs, uint32_t n, uint32_t dim, float* __restrict__ out) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gi = lane & 3u, r = lane >> 2;
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t base = warp * 8u; base < n; base += nwarps * 8u) {
+        const uint64_t row = base + r;
+        const bool valid = row < n;
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+        if (valid) {
+            const float* p = vecs + row * dim + 4u * gi;
+            for (uint32_t c = 0; c < dim; c += 16) {
+                const float4 v = __ldg(reinterpret_cast<const float4*>(p + c));
+                a0 = fmaf(v.x, v.x, a0);
+                a1 = fmaf(v.y, v.y, a1);
+                a2 = fmaf(v.z, v.z, a2);
+                a3 = fmaf(v.w, v.w, a3);
+            }
+        }
+        const float s = fold16<true>(a0, a1, a2, a3);
+        if (valid && gi == 0) out[row] = s;
+    }
+}
+
 // Sets *repeat when some level-0 row of at most 64 ids names an id twice; one
 // warp per vertex. Rows without repeats let the search take a whole row in one
 // pass (collect_row64_unique).
@@ -374,6 +403,7 @@ int fill_args(artea_gpu_router* r, SearchArgs* a, const float* d_q, uint32_t nq,
     const artea_gpu_index* ix = r->idx;
     std::memset(a, 0, sizeof(*a));
     a->g.vecs = ix->d_vecs;
+    a->g.xsq = ix->d_xsq;
     a->g.vinfo = ix->d_vinfo;
     a->g.nbrs = ix->d_nbrs;
     a->g.l0row = ix->d_l0row;
@@ -926,6 +956,24 @@ int index_begin(uint32_t num_vertices, const float* vectors, uint32_t num_vector
         return fail(ARTEA_GPU_ECUDA, "vector upload failed");
     }
     ix->bytes += sizeof(float) * nvec;
+    // x.x of every row, once, for the cosine distance.
+    if (int rc = dev_alloc(&ix->d_xsq, std::max(num_vectors, 1u))) {
+        artea_gpu_index_destroy(ix);
+        return rc;
+    }
+    ix->bytes += sizeof(float) * std::max(num_vectors, 1u);
+    if (num_vectors) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const uint32_t rows_per_block = 8u * 8u;   // 8 warps of 8 rows
+        const uint32_t blocks = std::min<uint32_t>((num_vectors + rows_per_block - 1) / rows_per_block,
+                                                   static_cast<uint32_t>(std::max(sms, 1)) * 16u);
+        row_sqnorm_kernel<<<blocks, 256>>>(ix->d_vecs, num_vectors, dim, ix->d_xsq);
+        if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+            artea_gpu_index_destroy(ix);
+            return fail(ARTEA_GPU_ECUDA, "row norms failed");
+        }
+    }
     *out = ix;
     return ARTEA_GPU_OK;
 }
@@ -1038,6 +1086,7 @@ int artea_gpu_index_destroy(artea_gpu_index* ix) {
     if (!ix) return ARTEA_GPU_OK;
     DeviceGuard guard(ix->device);
     dev_free(ix->d_vecs);
+    dev_free(ix->d_xsq);
     dev_free(ix->d_vinfo);
     dev_free(ix->d_nbrs);
     dev_free(ix->d_offsets);
@@ -1431,6 +1480,7 @@ extern "C" int artea_gpu_batch_query_noalloc(const artea_gpu_index* ix, int metr
     SearchArgs a;
     std::memset(&a, 0, sizeof(a));
     a.g.vecs = ix->d_vecs;
+    a.g.xsq = ix->d_xsq;
     a.g.vinfo = ix->d_vinfo;
     a.g.nbrs = ix->d_nbrs;
     a.g.l0row = ix->d_l0row;

@@ -26,6 +26,7 @@ struct artea_gpu_index {
     uint32_t l0_unique = 0;   // level-0 rows of <= 64 ids hold distinct ids (checked at upload)
     uint32_t nvecs = 0;       // vector rows uploaded (brute force scans all of them)
     float* d_vecs = nullptr;
+    float* d_xsq = nullptr;   // squared norm of every vector row (the cosine distance's x.x)
     uint2* d_vinfo = nullptr;
     uint32_t* d_nbrs = nullptr;
     uint64_t* d_offsets = nullptr;

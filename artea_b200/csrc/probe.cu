@@ -291,6 +291,7 @@ extern "C" int artea_gpu_subsystem_probe(const artea_gpu_index* ix, int metric, 
     SearchArgs a;
     std::memset(&a, 0, sizeof(a));
     a.g.vecs = ix->d_vecs;
+    a.g.xsq = ix->d_xsq;
     a.g.vinfo = ix->d_vinfo;
     a.g.nbrs = ix->d_nbrs;
     a.g.l0row = ix->d_l0row;

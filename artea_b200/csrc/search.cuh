@@ -53,6 +53,7 @@ constexpr uint32_t kWaitBound = 1u << 22;   // mbarrier polls before a copy coun
 
 struct DeviceGraph {
     const float* __restrict__ vecs;
+    const float* __restrict__ xsq;   // per-row x.x (row_sqnorm_kernel)
     const uint2* __restrict__ vinfo;
     const uint32_t* __restrict__ nbrs;
     const unsigned long long* __restrict__ l0row;
@@ -209,21 +210,17 @@ __device__ __forceinline__ float lo32(f32x2 v) { return __uint_as_float(static_c
 __device__ __forceinline__ float hi32(f32x2 v) { return __uint_as_float(static_cast<uint32_t>(v >> 32)); }
 
 // One chunk of 4 elements (x from the row, y from the query) into the pair
-// accumulators A01/A23 (and B01/B23 for cosine's x*x).
+// accumulators A01/A23.
 template <int kMetric>
-__device__ __forceinline__ void accumulate(const ulonglong2 x, const ulonglong2 y, f32x2& A01, f32x2& A23,
-                                           f32x2& B01, f32x2& B23) {
+__device__ __forceinline__ void accumulate(const ulonglong2 x, const ulonglong2 y, f32x2& A01, f32x2& A23) {
     if (kMetric == ARTEA_GPU_EUCLIDEAN_SQR || kMetric == ARTEA_GPU_EUCLIDEAN) {
         const f32x2 d01 = sub2(y.x, x.x), d23 = sub2(y.y, x.y);
         A01 = fma2(d01, d01, A01);
         A23 = fma2(d23, d23, A23);
     } else {
+        // dot and cosine: q.x (cosine's x.x comes from the index's row norms)
         A01 = fma2(y.x, x.x, A01);
         A23 = fma2(y.y, x.y, A23);
-        if (kMetric == ARTEA_GPU_COSINE) {
-            B01 = fma2(x.x, x.x, B01);
-            B23 = fma2(x.y, x.y, B23);
-        }
     }
 }
 
@@ -330,6 +327,9 @@ __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ 
         const uint32_t idx = p + r;
         const bool valid = idx < cnt;
         const uint32_t vid = valid ? cvid[idx] : 0u;
+        // x.x of the row, stored at index creation in this kernel's exact
+        // summation order (row_sqnorm_kernel); loaded ahead of the row.
+        const float xsq = (kMetric == ARTEA_GPU_COSINE && valid) ? __ldg(g.xsq + vid) : 1.0f;
         const float* row;
         if (kStage) {
             // The stage's previous contents have been read by every lane
@@ -353,7 +353,6 @@ __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ 
         }
         const float* qq = q + 4 * gi;
         f32x2 A01 = 0ull, A23 = 0ull;   // L2: diff^2; dot/cos: q*x   (+0.0f pairs)
-        f32x2 B01 = 0ull, B23 = 0ull;   // cos: x*x
         for (uint32_t cb = 0; cb < nchunks; cb += kBlock) {
             ulonglong2 x[kBlock];
             if (kPre && p == 0 && cb == 0) {
@@ -370,19 +369,17 @@ __device__ void batch_distances(const DeviceGraph& g, const float* __restrict__ 
             for (int k = 0; k < kBlock; ++k) {
                 if (cb + k < nchunks) {
                     const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(qq + 16 * (cb + k));
-                    accumulate<kMetric>(x[k], y, A01, A23, B01, B23);
+                    accumulate<kMetric>(x[k], y, A01, A23);
                 }
             }
         }
         const float a0 = lo32(A01), a1 = hi32(A01), a2 = lo32(A23), a3 = hi32(A23);
-        const float b0 = lo32(B01), b1 = hi32(B01), b2 = lo32(B23), b3 = hi32(B23);
         float res = fold16<kExact>(a0, a1, a2, a3);
         if (kMetric == ARTEA_GPU_EUCLIDEAN) {
             res = __fsqrt_rn(res);
         } else if (kMetric == ARTEA_GPU_DOT) {
             res = -res;
         } else if (kMetric == ARTEA_GPU_COSINE) {
-            const float xsq = fold16<kExact>(b0, b1, b2, b3);
             // utils/simd_distance.hpp:263-274
             const float denom = __fsqrt_rn(__fmul_rn(qsq, xsq));
             res = denom > 0.0f ? __fsub_rn(1.0f, __fdiv_rn(res, denom)) : 1.0f;

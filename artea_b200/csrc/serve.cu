@@ -220,6 +220,7 @@ int launch_serving(artea_gpu_server* s) {
     std::memset(&a, 0, sizeof(a));
     const artea_gpu_index* ix = s->idx;
     a.g.vecs = ix->d_vecs;
+    a.g.xsq = ix->d_xsq;
     a.g.vinfo = ix->d_vinfo;
     a.g.nbrs = ix->d_nbrs;
     a.g.l0row = ix->d_l0row;
