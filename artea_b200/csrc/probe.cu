@@ -153,9 +153,8 @@ __global__ void __launch_bounds__(kProbeBudgetThreads, 5) probe_queue_kernel(Sea
     const uint32_t qw = queue_words(a.cap);
     float* base = smem + static_cast<size_t>(warp) * (2 * qw + 4 * kCandBatch);
     Queue q;
-    q.d = base;
-    q.v = reinterpret_cast<uint32_t*>(base + qw);
-    uint32_t* cvid = q.v + qw;
+    q.e = reinterpret_cast<uint2*>(base);
+    uint32_t* cvid = reinterpret_cast<uint32_t*>(base + 2 * qw);
     float* cdist = reinterpret_cast<float*>(cvid + kCandBatch);
     float* bd = cdist + kCandBatch;
     uint32_t* bv = reinterpret_cast<uint32_t*>(bd + kCandBatch);
@@ -179,7 +178,7 @@ __global__ void __launch_bounds__(kProbeBudgetThreads, 5) probe_queue_kernel(Sea
             int p2;
             const int pi = queue_pop_peek(q, &p2);
             const uint2 rec = rows[r];
-            if (pi < 0 || (q.v[pi] & kVidMask) != rec.x) {
+            if (pi < 0 || (q.e[pi].x & kVidMask) != rec.x) {
                 ++bad;
                 break;
             }

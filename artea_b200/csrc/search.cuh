@@ -506,59 +506,66 @@ struct Visited {
     uint32_t spills;
 };
 
-// One id's walk through the table: the bucket to read, the slot value looked
-// for (and inserted), and the second bucket while it is still to come.
+// One id's place in the table: its first bucket, its second (~0u when the
+// quotient leaves no second choice) and its quotient.
 struct TableWalk {
-    uint32_t bucket;
-    uint32_t val;
-    uint32_t alt;       // the second bucket, or ~0u when there is none
+    uint32_t a;
+    uint32_t b;
+    uint32_t q;
 };
 
 __device__ __forceinline__ TableWalk table_walk(const Visited& vs, uint32_t vid) {
     const uint32_t p = (vid * kVisitedMul) & vs.kmask;
     const uint32_t qbits = vs.kbits - vs.tbits;
     TableWalk w;
-    w.bucket = p >> qbits;
-    const uint32_t q = p & ((1u << qbits) - 1u);
-    w.val = q;
+    w.a = p >> qbits;
+    w.q = p & ((1u << qbits) - 1u);
     // alt(Q): the second bucket's offset from the quotient's bits (0 would
     // give B == A: no second choice for that quotient).
-    const uint32_t h = (q * 0x2545F491u) >> (32u - vs.tbits);
-    w.alt = (qbits <= 14 && h != 0) ? (w.bucket ^ h) : 0xffffffffu;
+    const uint32_t h = (w.q * 0x2545F491u) >> (32u - vs.tbits);
+    w.b = (qbits <= 14 && h != 0) ? (w.a ^ h) : 0xffffffffu;
     return w;
 }
 
-// One bucket read (and at most one CAS) of a walk: -1 while the walk goes on,
-// else 1 (the id is present), 0 (inserted now) or 2 (its buckets are full:
-// the bitset decides).
-__device__ __forceinline__ int table_step(const Visited& vs, TableWalk& w) {
-    const uint2 b = vs.tab[w.bucket];
-    const uint32_t pair = w.val | (w.val << 16);
-    if (__vcmpeq2(b.x, pair) | __vcmpeq2(b.y, pair)) return 1;
-    const uint32_t e0 = __vcmpeq2(b.x, 0xFFFFFFFFu), e1 = __vcmpeq2(b.y, 0xFFFFFFFFu);
+// Both buckets read at once (at most one CAS): 1 if the id is present (Q in
+// A, or Q | flag in B), 0 if it was inserted now (into A while A has a free
+// slot, else into B), 2 if both are full (the bitset decides), -1 if another
+// lane filled the chosen slot meanwhile (read again). A match in B is the id
+// itself whatever A holds: (B, Q) gives back A.
+__device__ __forceinline__ int table_try(const Visited& vs, const TableWalk& w) {
+    const bool has_b = w.b != 0xffffffffu;
+    const uint2 ba = vs.tab[w.a];
+    const uint2 bb = has_b ? vs.tab[w.b] : make_uint2(0u, 0u);   // no empty slot, no flagged value
+    const uint32_t fq = w.q | kAltFlag;
+    const uint32_t pa = w.q | (w.q << 16), pb = fq | (fq << 16);
+    if (__vcmpeq2(ba.x, pa) | __vcmpeq2(ba.y, pa) | __vcmpeq2(bb.x, pb) | __vcmpeq2(bb.y, pb)) return 1;
+    uint32_t e0 = __vcmpeq2(ba.x, 0xFFFFFFFFu), e1 = __vcmpeq2(ba.y, 0xFFFFFFFFu);
+    uint32_t bucket = w.a, val = w.q;
+    uint2 bk = ba;
     if (!(e0 | e1)) {
-        if (w.alt == 0xffffffffu) return 2;
-        // The first bucket is full: the second decides.
-        w.bucket = w.alt;
-        w.val |= kAltFlag;
-        w.alt = 0xffffffffu;
-        return -1;
+        // A is full (for good): B decides.
+        e0 = __vcmpeq2(bb.x, 0xFFFFFFFFu);
+        e1 = __vcmpeq2(bb.y, 0xFFFFFFFFu);
+        if (!(e0 | e1)) return 2;
+        bucket = w.b;
+        val = fq;
+        bk = bb;
     }
     const int wi = e0 ? 0 : 1;
-    const uint32_t old = e0 ? b.x : b.y;
+    const uint32_t old = e0 ? bk.x : bk.y;
     const uint32_t e = e0 ? e0 : e1;
-    const uint32_t desired = (e & 0xFFFFu) ? ((old & 0xFFFF0000u) | w.val) : ((old & 0x0000FFFFu) | (w.val << 16));
-    uint32_t* word = reinterpret_cast<uint32_t*>(vs.tab + w.bucket) + wi;
-    if (atomicCAS(word, old, desired) == old) return 0;
-    return -1;   // another lane filled that slot meanwhile: read the bucket again
+    const uint32_t desired = (e & 0xFFFFu) ? ((old & 0xFFFF0000u) | val) : ((old & 0x0000FFFFu) | (val << 16));
+    uint32_t* word = reinterpret_cast<uint32_t*>(vs.tab + bucket) + wi;
+    return atomicCAS(word, old, desired) == old ? 0 : -1;
 }
 
 // Returns 1 if vid is in the table, 0 if it was inserted now, 2 if its
-// buckets are full (the bitset decides).
+// buckets are full (the bitset decides). Every retry follows a slot filled
+// by another lane, so the loop ends within the 8 slots of the two buckets.
 __device__ __forceinline__ int table_test_insert(const Visited& vs, uint32_t vid) {
-    TableWalk w = table_walk(vs, vid);
+    const TableWalk w = table_walk(vs, vid);
     for (int step = 0; step < 24; ++step) {
-        const int r = table_step(vs, w);
+        const int r = table_try(vs, w);
         if (r >= 0) return r;
     }
     return 2;
@@ -603,11 +610,11 @@ __device__ __forceinline__ void visited_set(Visited& vs, uint32_t vid) {
 // interleaved. r0/r1 as table_test_insert's return values (-1: inactive).
 __device__ __forceinline__ void table_test_insert2(const Visited& vs, uint32_t v0, bool a0, uint32_t v1, bool a1,
                                                    int* r0, int* r1) {
-    TableWalk w0 = table_walk(vs, a0 ? v0 : 0u), w1 = table_walk(vs, a1 ? v1 : 0u);
+    const TableWalk w0 = table_walk(vs, a0 ? v0 : 0u), w1 = table_walk(vs, a1 ? v1 : 0u);
     int t0 = a0 ? -1 : -2, t1 = a1 ? -1 : -2;
     for (int step = 0; step < 24 && (t0 == -1 || t1 == -1); ++step) {
-        if (t0 == -1) t0 = table_step(vs, w0);
-        if (t1 == -1) t1 = table_step(vs, w1);
+        if (t0 == -1) t0 = table_try(vs, w0);
+        if (t1 == -1) t1 = table_try(vs, w1);
     }
     *r0 = a0 ? (t0 < 0 ? 2 : t0) : -1;
     *r1 = a1 ? (t1 < 0 ? 2 : t1) : -1;
@@ -730,15 +737,16 @@ __device__ __forceinline__ uint32_t collect_row64_unique(const DeviceGraph& g, V
 
 // ---------------------------------------------------------------------------
 // Candidate queue (subsystem b). Sorted ascending by (dist, vid) in shared
-// memory; bit 31 of the vid word marks "explored". T = the first min(n, L)
+// memory, one 8-byte entry {vid word, dist bits} per candidate, so a search
+// step, a move or a pop test is one load; bit 31 of the vid word marks
+// "explored". T = the first min(n, L)
 // entries. Entries past L that tie the worst distance lb are entries the
 // reference evicted from its top-L heap but still holds in its unexplored
 // heap; they stay expandable until lb drops. Any entry worse than lb is dead
 // and trimmed. At most L entries can tie lb, so 2L slots always suffice.
 // ---------------------------------------------------------------------------
 struct Queue {
-    float* d;
-    uint32_t* v;
+    uint2* e;        // entries {vid word, dist bits}: one 8-byte access per entry
     uint32_t n;
     uint32_t L;
     uint32_t cap;
@@ -746,13 +754,20 @@ struct Queue {
     float lb;        // d[L-1] once n >= L
 };
 
+__device__ __forceinline__ float ent_d(uint2 w) { return __uint_as_float(w.y); }
+__device__ __forceinline__ uint2 make_ent(float d, uint32_t v) { return make_uint2(v, __float_as_uint(d)); }
+
 __device__ __forceinline__ uint32_t queue_lower_bound(const Queue& q, float d, uint32_t v) {
     const int lane = lane_id();
     uint32_t lo = 0, hi = q.n;
     while (hi - lo > 32) {
         const uint32_t step = (hi - lo + 31) / 32;
         const uint32_t idx = lo + lane * step;
-        const bool less = idx < hi && entry_less(q.d[idx], q.v[idx], d, v);
+        bool less = false;
+        if (idx < hi) {
+            const uint2 w = q.e[idx];
+            less = entry_less(ent_d(w), w.x, d, v);
+        }
         const int c = __popc(__ballot_sync(kFull, less));
         const uint32_t new_lo = c == 0 ? lo : lo + (c - 1) * step + 1;
         const uint32_t new_hi = min(hi, lo + c * step);
@@ -760,7 +775,11 @@ __device__ __forceinline__ uint32_t queue_lower_bound(const Queue& q, float d, u
         hi = new_hi;
     }
     const uint32_t idx = lo + lane;
-    const bool less = idx < hi && entry_less(q.d[idx], q.v[idx], d, v);
+    bool less = false;
+    if (idx < hi) {
+        const uint2 w = q.e[idx];
+        less = entry_less(ent_d(w), w.x, d, v);
+    }
     return lo + __popc(__ballot_sync(kFull, less));
 }
 
@@ -776,24 +795,23 @@ __device__ __forceinline__ bool queue_insert(Queue& q, float d, uint32_t v, int*
         const int s = max(static_cast<int>(pos), end - 32);
         const int idx = s + lane;
         const bool act = idx < end;
-        float dd = 0.f;
-        uint32_t vv = 0;
-        if (act) { dd = q.d[idx]; vv = q.v[idx]; }
+        uint2 ww = make_uint2(0u, 0u);
+        if (act) ww = q.e[idx];
         __syncwarp();
-        if (act) { q.d[idx + 1] = dd; q.v[idx + 1] = vv; }
+        if (act) q.e[idx + 1] = ww;
         __syncwarp();
     }
-    if (lane == 0) { q.d[pos] = d; q.v[pos] = v & kVidMask; }
+    if (lane == 0) q.e[pos] = make_ent(d, v & kVidMask);
     __syncwarp();
     q.n++;
     if (pos < q.hint) q.hint = pos;
     if (q.n >= q.L) {
-        q.lb = q.d[q.L - 1];
+        q.lb = ent_d(q.e[q.L - 1]);
         if (q.n > q.L) {
             uint32_t newn = q.n;
             for (uint32_t base = q.L; base < q.n; base += 32) {
                 const uint32_t idx = base + lane;
-                const bool dead = idx < q.n && q.d[idx] > q.lb;
+                const bool dead = idx < q.n && ent_d(q.e[idx]) > q.lb;
                 const uint32_t b = __ballot_sync(kFull, dead);
                 if (b) { newn = base + __ffs(b) - 1; break; }
             }
@@ -808,7 +826,7 @@ __device__ __forceinline__ int queue_find_unexplored(const Queue& q, uint32_t fr
     const int lane = lane_id();
     for (uint32_t base = from; base < q.n; base += 32) {
         const uint32_t idx = base + lane;
-        const bool un = idx < q.n && !(q.v[idx] & kExplored);
+        const bool un = idx < q.n && !(q.e[idx].x & kExplored);
         const uint32_t b = __ballot_sync(kFull, un);
         if (b) return static_cast<int>(base + __ffs(b) - 1);
     }
@@ -824,7 +842,7 @@ __device__ __forceinline__ int queue_pop(Queue& q) {
         q.hint = q.n;
         return -1;
     }
-    if (lane_id() == 0) q.v[p] |= kExplored;
+    if (lane_id() == 0) q.e[p].x |= kExplored;
     __syncwarp();
     q.hint = static_cast<uint32_t>(p) + 1;
     return p;
@@ -839,7 +857,7 @@ __device__ __forceinline__ int queue_pop_peek(Queue& q, int* next) {
     uint32_t base = q.hint;
     for (; base < q.n; base += 32) {
         const uint32_t idx = base + lane;
-        const bool un = idx < q.n && !(q.v[idx] & kExplored);
+        const bool un = idx < q.n && !(q.e[idx].x & kExplored);
         uint32_t b = __ballot_sync(kFull, un);
         if (b) {
             if (first < 0) {
@@ -856,7 +874,7 @@ __device__ __forceinline__ int queue_pop_peek(Queue& q, int* next) {
         q.hint = q.n;
         return -1;
     }
-    if (lane == 0) q.v[first] |= kExplored;
+    if (lane == 0) q.e[first].x |= kExplored;
     __syncwarp();
     q.hint = static_cast<uint32_t>(first) + 1;
     return first;
@@ -906,7 +924,7 @@ __device__ inline uint32_t queue_accept(const Queue& q, const uint32_t* cvid, co
         bool acc = false;
         if (improving && ub < q.L) {
             const uint32_t idx = q.L - ub - 1;
-            acc = idx >= tn || q.d[idx] > d;
+            acc = idx >= tn || ent_d(q.e[idx]) > d;
         }
         const bool undecided = improving && !acc && ub != 0;
         if (__any_sync(kFull, undecided)) {
@@ -928,7 +946,7 @@ __device__ inline uint32_t queue_accept(const Queue& q, const uint32_t* cvid, co
             }
             if (undecided && pre < q.L) {
                 const uint32_t idx = q.L - pre - 1;
-                acc = idx >= tn || q.d[idx] > d;
+                acc = idx >= tn || ent_d(q.e[idx]) > d;
             }
         }
         const uint32_t b = __ballot_sync(kFull, acc);
@@ -949,7 +967,8 @@ __device__ __forceinline__ uint32_t old_lower_bound(const Queue& q, float d, uin
     uint32_t lo = 0, hi = q.n;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (entry_less(q.d[mid], q.v[mid], d, v)) lo = mid + 1; else hi = mid;
+        const uint2 w = q.e[mid];
+        if (entry_less(ent_d(w), w.x, d, v)) lo = mid + 1; else hi = mid;
     }
     return lo;
 }
@@ -1022,28 +1041,21 @@ __device__ inline bool queue_merge(Queue& q, float* bd, uint32_t* bv, uint32_t m
         const int o = cb + lane;
         const bool act = o >= p0;
         const bool from_batch = (mask >> lane) & 1u;
-        float dd = 0.f;
-        uint32_t vv = 0u;
-        if (act) {
-            dd = from_batch ? bd[before] : q.d[o - before];
-            vv = from_batch ? bv[before] : q.v[o - before];
-        }
+        uint2 ww = make_uint2(0u, 0u);
+        if (act) ww = from_batch ? make_ent(bd[before], bv[before]) : q.e[o - before];
         __syncwarp();
-        if (act) {
-            q.d[o] = dd;
-            q.v[o] = vv;
-        }
+        if (act) q.e[o] = ww;
     }
     __syncwarp();
     const uint32_t total = min(q.n + m, q.cap);
     q.n = total;
     if (static_cast<uint32_t>(p0) < q.hint) q.hint = static_cast<uint32_t>(p0);
     if (q.n >= q.L) {
-        q.lb = q.d[q.L - 1];
+        q.lb = ent_d(q.e[q.L - 1]);
         uint32_t newn = q.n;
         for (uint32_t base = q.L; base < q.n; base += 32) {
             const uint32_t idx = base + lane;
-            const bool dead = idx < q.n && q.d[idx] > q.lb;
+            const bool dead = idx < q.n && ent_d(q.e[idx]) > q.lb;
             const uint32_t b = __ballot_sync(kFull, dead);
             if (b) { newn = base + __ffs(b) - 1; break; }
         }
@@ -1157,8 +1169,7 @@ struct WarpSmem {
     unsigned long long* mbar;    // staging mbarrier (null without staging)
     float* stage;                // staged rows, 16-byte aligned (null without staging)
     float* q;
-    float* qd;
-    uint32_t* qv;
+    uint2* qe;
     uint32_t* cvid;
     float* cdist;
     float* bd;
@@ -1173,9 +1184,8 @@ __device__ __forceinline__ WarpSmem carve(float* base, uint32_t dim, uint32_t ca
     s.mbar = stage_rows ? reinterpret_cast<unsigned long long*>(base + kPhaseWords) : nullptr;
     s.stage = stage_rows ? base + kPhaseWords + 4 : nullptr;
     s.q = base + kPhaseWords + stage_words(dim, stage_rows);
-    s.qd = s.q + dim;
-    s.qv = reinterpret_cast<uint32_t*>(s.qd + queue_words(cap));
-    s.cvid = s.qv + queue_words(cap);
+    s.qe = reinterpret_cast<uint2*>(s.q + dim);
+    s.cvid = reinterpret_cast<uint32_t*>(s.q + dim + 2 * queue_words(cap));
     s.cdist = reinterpret_cast<float*>(s.cvid + kCandBatch);
     s.bd = s.cdist + kCandBatch;
     s.bv = reinterpret_cast<uint32_t*>(s.bd + kCandBatch);
@@ -1217,7 +1227,7 @@ __device__ __forceinline__ bool l0_search_pipelined(const SearchArgs& a, Queue& 
     uint32_t* cv = sm.cvid;
     float* cd = sm.cdist;
     // Pop the cursor: the queue's only entry.
-    if (lane == 0) q.v[0] |= kExplored;
+    if (lane == 0) q.e[0].x |= kExplored;
     __syncwarp();
     q.hint = 1;
     unsigned long long desc = __ldg(g.l0row + cur);
@@ -1259,15 +1269,15 @@ __device__ __forceinline__ bool l0_search_pipelined(const SearchArgs& a, Queue& 
             float bdm;
             uint32_t bvm;
             const uint32_t bi = batch_argmin(sm.bd, sm.bv, m, &bdm, &bvm);
-            take_new = p2 < 0 || entry_less(bdm, bvm, q.d[p2], q.v[p2]);
+            take_new = p2 < 0 || entry_less(bdm, bvm, ent_d(q.e[p2]), q.e[p2].x);
             if (take_new) {
                 next = bvm & kVidMask;
                 if (lane == 0) sm.bv[bi] = bvm | kExplored;
             }
         }
         if (!take_new && p2 >= 0) {
-            next = q.v[p2] & kVidMask;
-            if (lane == 0) q.v[p2] |= kExplored;
+            next = q.e[p2].x & kVidMask;
+            if (lane == 0) q.e[p2].x |= kExplored;
             q.hint = static_cast<uint32_t>(p2) + 1;
         }
         __syncwarp();
@@ -1307,7 +1317,7 @@ __device__ __forceinline__ bool l0_search_pipelined(const SearchArgs& a, Queue& 
         p2 = queue_find_unexplored(q, q.hint);
         if (p2 >= 0) {
             q.hint = static_cast<uint32_t>(p2);
-            pf_vid = q.v[p2] & kVidMask;
+            pf_vid = q.e[p2].x & kVidMask;
             pf_desc = __ldg(g.l0row + pf_vid);
         } else {
             q.hint = q.n;
@@ -1444,8 +1454,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
 
         // Level-0 beam search (single_layer_router.hpp:145-163, beam_loop.hpp:90-119).
         Queue q;
-        q.d = sm.qd;
-        q.v = sm.qv;
+        q.e = sm.qe;
         q.n = 0;
         q.L = L;
         q.cap = a.cap;
@@ -1473,7 +1482,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                 int p2;
                 const int p = queue_pop_peek(q, &p2);
                 if (p < 0) break;
-                const uint32_t v = q.v[p] & kVidMask;
+                const uint32_t v = q.e[p].x & kVidMask;
                 if (v == kVidMask) break;   // CandidateEntry::is_invalid
                 const bool hit = v == pf_vid;
                 if (hit) pc.count(kPhPrefetchHits);
@@ -1490,7 +1499,7 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
                 }
                 pf_have_ids = false;
                 if (p2 >= 0) {
-                    pf_vid = q.v[p2] & kVidMask;
+                    pf_vid = q.e[p2].x & kVidMask;
                     pf_desc = __ldg(g.l0row + pf_vid);
                 } else {
                     pf_vid = kVidMask;
@@ -1566,7 +1575,8 @@ __device__ void search_one(const SearchArgs& a, uint32_t qi, uint32_t slot, cons
         for (uint32_t i = lane; i < a.k_stride; i += 32) {
             uint64_t w = kInvalidWord;
             if (i < nres) {
-                w = (static_cast<uint64_t>(__float_as_uint(sm.qd[i])) << 32) | (sm.qv[i] & kVidMask);
+                const uint2 e = sm.qe[i];
+                w = (static_cast<uint64_t>(e.y) << 32) | (e.x & kVidMask);
             }
             out[i] = w;
         }
