@@ -18,6 +18,10 @@ Workloads (name -> shape):
   {64, 128, 256, 512}.
 * ``gist1m``: 1,000,000 x 960 L2, 512 centres U[0, 0.3]^960, sigma 0.05,
   clipped at 0; 1,000 queries; queue in {200, 400}; l0_min_distance 0.05.
+* ``deep1m410``: deep10m's generator with 1,000,000 base vectors and 410
+  centres (the 10M index's 2,439 vectors per cluster), 10,000 queries and the
+  same per-query topk/queue draws: the 10M workload's search behaviour at a
+  tenth of the graph build.
 
 Any workload can be scaled down (``n_base``/``n_query`` overrides) for tests.
 """
@@ -68,6 +72,11 @@ WORKLOADS = {
                         topk=100, queue=512),
     "gist1m": Workload("gist1m", 1_000_000, 1_000, 960, METRIC_L2, 512, "gist", 1003,
                        queue=400, l0_min_distance=0.05),
+    # deep10m's generator and queries at 1/10 of the base with 1/10 of the
+    # centres: the same 2,439 vectors per cluster, so a search does what it
+    # does on the 10M index, on a graph that builds in minutes.
+    "deep1m410": Workload("deep1m410", 1_000_000, 10_000, 96, METRIC_COSINE, 410, "deep", 1002,
+                          topk=100, queue=512),
 }
 
 _STREAM_CENTRES, _STREAM_BASE, _STREAM_QUERY, _STREAM_PARAMS = 0, 1, 2, 3

@@ -863,6 +863,9 @@ def main() -> None:
     ap.add_argument("--profile-slack", type=int, default=0, help="compact queue slack (0: 2L layout)")
     ap.add_argument("--profile-wpq", type=int, default=1, help="warps per query")
     ap.add_argument("--phases", action="store_true", help="with --profile: per-phase cycle breakdown")
+    ap.add_argument("--profile-nq", type=int, default=0, help="with --profile: the batch's first N queries only")
+    ap.add_argument("--profile-only-queue", type=int, default=0,
+                    help="with --profile on per-query queues: only the queries drawn with this queue size")
     ap.add_argument("--probe", action="store_true",
                     help="subsystem probes at --profile-queue: the search traced, then the greedy descent, distance "
                          "gathers, visited set and queue replayed alone (artea_gpu_subsystem_probe)")
@@ -973,11 +976,19 @@ def run_profile(args, w, queries, index, metric, device):
     import torch
     from artea_b200.router import GpuRouter
     nq, k = queries.shape[0], w.topk
+    topk_all, queue_all = ds.per_query_params(w, nq)
+    if args.profile_only_queue:
+        keep = np.nonzero(queue_all == args.profile_only_queue)[0]
+        queries, topk_all, queue_all = queries[keep], topk_all[keep], queue_all[keep]
+        nq = len(keep)
+    if args.profile_nq:
+        nq = min(nq, args.profile_nq)
+        queries = np.ascontiguousarray(queries[:nq])
     d_q = torch.from_numpy(queries).to(device)
     d_tk = d_qu = None
     L = args.profile_queue
     if args.uneven or w.kind == "deep":
-        topk, queue = ds.per_query_params(w, nq)
+        topk, queue = np.ascontiguousarray(topk_all[:nq]), np.ascontiguousarray(queue_all[:nq])
         k, L = int(topk.max()), int(queue.max())
         d_tk = torch.from_numpy(topk.view(np.int32)).to(device)
         d_qu = torch.from_numpy(queue.view(np.int32)).to(device)
@@ -992,17 +1003,24 @@ def run_profile(args, w, queries, index, metric, device):
                   queue_slack=args.profile_slack or 0xFFFFFFFF, warps_per_query=args.profile_wpq)
     s = torch.cuda.current_stream(device)
     phases = torch.zeros((nq, 8), dtype=torch.int64, device=device) if args.phases else None
+    d_stats = torch.zeros((nq, 8), dtype=torch.int32, device=device)
+    times = []
     for rep in range(2):
         if phases is not None and rep == 1:
             r.set_phase_buffer(phases)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        r.batch_query_device(d_q, nq, k, d_out, d_topk=d_tk, d_queue=d_qu, stream=s.cuda_stream)
+        r.batch_query_device(d_q, nq, k, d_out, d_topk=d_tk, d_queue=d_qu, d_stats=d_stats if rep == 0 else None,
+                             stream=s.cuda_stream)
         e1.record(s)
         torch.cuda.synchronize(device)
-        log(f"profile launch: {e0.elapsed_time(e1):.3f} ms for {nq} queries")
+        times.append(e0.elapsed_time(e1))
+        log(f"profile launch: {times[-1]:.3f} ms for {nq} queries")
     r.sync()
-    out = {"tuning": r.tuning()}
+    st = d_stats.cpu().numpy().view(np.uint32)
+    out = {"tuning": r.tuning(), "queries": nq, "ms": times[-1],
+           "per_query": {"dist_evals": float(st[:, 0].mean()), "l0_rows": float(st[:, 3].mean()),
+                         "l0_rows_max": int(st[:, 3].max())}}
     if phases is not None:
         ph = phases.cpu().numpy().astype(np.float64)
         names = ["upper", "pop_row", "ids_visited", "distances", "merge", "tail", "total", "prefetch_hits"]
