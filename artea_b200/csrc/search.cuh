@@ -1152,10 +1152,11 @@ __host__ __device__ inline uint32_t stage_words(uint32_t dim, uint32_t stage_row
     return stage_rows ? 4u + stage_rows * (dim + kStagePad) : 0u;
 }
 
-// The queue's two arrays take an even number of entries each, so that the
-// regions after them (the 16-byte visited buckets, the next warp's area)
-// stay 16-byte aligned whatever the capacity (dim, the stage and the fixed
-// parts are multiples of 4 words).
+// The queue's entry array holds an even number of 8-byte entries
+// (2 * queue_words(cap) words), so that the regions after it (the visited
+// table, read 16 bytes at a time when cleared, the next warp's area) stay
+// 16-byte aligned whatever the capacity (dim, the stage and the fixed parts
+// are multiples of 4 words).
 __host__ __device__ inline uint32_t queue_words(uint32_t cap) { return (cap + 1u) & ~1u; }
 
 __host__ __device__ inline uint32_t warp_smem_words(uint32_t dim, uint32_t cap, uint32_t vh_bits,
