@@ -228,7 +228,7 @@ int artea_gpu_index_create_from_hgra(const char* path, const float* vectors, uin
 int artea_gpu_index_download(const artea_gpu_index* index, uint32_t* vertex_info, uint64_t* offsets,
                              uint32_t* neighbor_ids);
 int artea_gpu_index_destroy(artea_gpu_index* index);
-/* Device bytes held by the index (vectors + CSR). */
+/* Device bytes held by the index (vectors, their x.x row norms, CSR). */
 int artea_gpu_index_bytes(const artea_gpu_index* index, uint64_t* bytes);
 
 /* ---- Router ---- */
