@@ -184,3 +184,52 @@ def test_gather_merge_moves_equal_a_sorted_merge(seed):
         keys = [(float(d), int(v)) for d, v in zip(rng.integers(0, 40, n + m), rng.permutation(100000)[: n + m])]
         old, batch = sorted(keys[:n]), keys[n:]
         assert gather_merge(old, batch, cap) == sorted(keys)[: min(n + m, cap)]
+
+
+class BatchedRecording(Batched):
+    """Batched, keeping the row's accepted candidates for the next-pop rule."""
+
+    def push_row(self, row):
+        L, A = self.L, self.A
+        tn = min(len(A), L)
+        lim = self.lb if len(A) >= L else INF
+        self.last_accepted = []
+        for j, (d, v) in enumerate(row):
+            if not d < lim:
+                continue
+            pre = sum(1 for i in range(j) if row[i][0] < lim and row[i][0] <= d)
+            if pre < L and (L - pre - 1 >= tn or A[L - pre - 1][0] > d):
+                self.last_accepted.append((d, v))
+        super().push_row(row)
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_next_pop_is_min_of_p2_and_smallest_accepted(seed):
+    # The pipelined level-0 loop (l0_search_pipelined) decides the next pop right
+    # after acceptance, before the merge: min(p2, smallest accepted candidate),
+    # p2 being the first unexplored entry once the current one is popped; with
+    # neither, the search ends. Checked against the merged queue's actual pop on
+    # beam-search sequences (pop, push its row, pop, ...).
+    rng = np.random.default_rng(3000 + seed)
+    for _ in range(300):
+        L = int(rng.integers(1, 12))
+        q, used = BatchedRecording(L), set()
+        first = (float(rng.integers(0, 8)), int(rng.integers(0, 400)))
+        used.add(first[1])
+        q.A.append([first[0], first[1], False])
+        for _ in range(int(rng.integers(3, 40))):
+            cur = q.pop()
+            if cur is None:
+                break
+            p2 = next(((e[0], e[1]) for e in q.A if not e[2]), None)
+            row = []
+            for _ in range(int(rng.integers(0, 70))):
+                v = int(rng.integers(0, 400))
+                if v not in used:
+                    used.add(v)
+                    row.append((float(rng.integers(0, int(rng.integers(2, 12)))), v))
+            q.push_row(row)
+            options = [e for e in ([p2] if p2 else []) + ([min(q.last_accepted)] if q.last_accepted else [])]
+            predicted = min(options) if options else None
+            actual = next(((e[0], e[1]) for e in q.A if not e[2]), None)
+            assert predicted == actual, (L, cur, p2, q.last_accepted, actual)
