@@ -977,6 +977,9 @@ def run_profile(args, w, queries, index, metric, device):
     from artea_b200.router import GpuRouter
     nq, k = queries.shape[0], w.topk
     topk_all, queue_all = ds.per_query_params(w, nq)
+    per_query = args.uneven or w.kind == "deep"
+    if args.profile_only_queue and not per_query:
+        raise SystemExit("--profile-only-queue needs per-query queue sizes (a deep workload or --uneven)")
     if args.profile_only_queue:
         keep = np.nonzero(queue_all == args.profile_only_queue)[0]
         queries, topk_all, queue_all = queries[keep], topk_all[keep], queue_all[keep]
@@ -987,7 +990,7 @@ def run_profile(args, w, queries, index, metric, device):
     d_q = torch.from_numpy(queries).to(device)
     d_tk = d_qu = None
     L = args.profile_queue
-    if args.uneven or w.kind == "deep":
+    if per_query:
         topk, queue = np.ascontiguousarray(topk_all[:nq]), np.ascontiguousarray(queue_all[:nq])
         k, L = int(topk.max()), int(queue.max())
         d_tk = torch.from_numpy(topk.view(np.int32)).to(device)
